@@ -1,0 +1,194 @@
+// Shared device helpers of the cone-beam library: storage types, the
+// texture-compatible interpolation weights and error reporting.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "kk.h"
+
+namespace kk {
+
+// ---------------------------------------------------------------------------
+// storage types: every kernel accumulates in float32 whatever it stores
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ float ld(const T* p);
+template <>
+__device__ __forceinline__ float ld<float>(const float* p) { return __ldg(p); }
+template <>
+__device__ __forceinline__ float ld<__nv_bfloat16>(const __nv_bfloat16* p) {
+    return __bfloat162float(__ldg(p));
+}
+template <>
+__device__ __forceinline__ float ld<__half>(const __half* p) { return __half2float(__ldg(p)); }
+
+// plain (coherent) load for data the same kernel may write
+template <typename T>
+__device__ __forceinline__ float ld_rw(const T* p);
+template <>
+__device__ __forceinline__ float ld_rw<float>(const float* p) { return *p; }
+template <>
+__device__ __forceinline__ float ld_rw<__nv_bfloat16>(const __nv_bfloat16* p) {
+    return __bfloat162float(*p);
+}
+template <>
+__device__ __forceinline__ float ld_rw<__half>(const __half* p) { return __half2float(*p); }
+
+template <typename T>
+__device__ __forceinline__ void st(T* p, float v);
+template <>
+__device__ __forceinline__ void st<float>(float* p, float v) { *p = v; }
+template <>
+__device__ __forceinline__ void st<__nv_bfloat16>(__nv_bfloat16* p, float v) {
+    *p = __float2bfloat16_rn(v);
+}
+template <>
+__device__ __forceinline__ void st<__half>(__half* p, float v) { *p = __float2half_rn(v); }
+
+// ---------------------------------------------------------------------------
+// interpolation weights
+// ---------------------------------------------------------------------------
+// CUDA's linear texture filtering (unnormalised coordinates, border
+// addressing) reads texels floor(x - 0.5) and floor(x - 0.5) + 1.
+// KK_INTERP_TEX8 reproduces the filter of the B200 texture unit the
+// reference samples with, as measured by the texture-probe golden vectors
+// (tests/test_texture_model.py):
+//   * each coordinate is rounded half-up onto a 1/256 grid before it is
+//     split, so the per-axis weight is an integer A in [0, 255] (units of
+//     1/256) and a weight that rounds up to 1 moves to the next texel;
+//   * the bilinear weights are w11 = round_half_up(A1 * A2 / 256),
+//     w10 = A1 - w11, w01 = A2 - w11, w00 = 256 - A1 - A2 + w11, i.e. the
+//     four product weights on the same 1/256 grid, summing to exactly 1.
+// KK_INTERP_EXACT splits the float32 coordinate exactly and interpolates
+// separably.
+//
+// Coordinates are clamped to +-2^15 first: far outside any array every
+// texel is a border zero either way, the clamp keeps the integer
+// conversion defined (non-finite values land on a border too), and below
+// 2^15 the half-up rounding x * 256 + 0.5 is exact. Arrays are therefore
+// limited to 32767 texels per axis (checked on the host).
+constexpr float COORD_LIMIT = 32768.f;
+
+struct Split {
+    int i;    // left texel
+    float w;  // weight of texel i + 1: integer 0..255 (TEX8) or [0, 1)
+};
+
+template <bool TEX8>
+__device__ __forceinline__ Split split_coord(float x) {
+    x = fminf(fmaxf(x, -COORD_LIMIT), COORD_LIMIT);
+    Split s;
+    if (TEX8) {
+        const float q = floorf(x * 256.f + 0.5f) - 128.f;  // exact below 2^15
+        const float fi = floorf(q * (1.f / 256.f));
+        s.i = (int)fi;
+        s.w = q - fi * 256.f;
+    } else {
+        const float xb = x - 0.5f;
+        const float fi = floorf(xb);
+        s.i = (int)fi;
+        s.w = xb - fi;
+    }
+    return s;
+}
+
+// Weights of a bilinear footprint, indexed [a][b] by the left/right texel
+// along the two axes. For KK_INTERP_TEX8 they are the texture unit's
+// weights in units of 1/256 (measured on the B200 by the texture-probe
+// golden vectors, tests/test_texture_model.py); A, B are the per-axis
+// weights from split_coord:
+//   rule 0: 2D arrays, and the plane of the two fastest axes of a 3D array:
+//           w11 = round_half_up(A B / 256), the other three derived so the
+//           marginals stay A and B;
+//   rule 1: fastest + slowest axis of a 3D array: each slice of the slow
+//           axis (weights 256 - S, S) is split along the fast axis with
+//           round_half_up(F * slice / 256) for the right fast texel;
+//   rule 2: middle + slowest axis: the same split anchored on the left
+//           fast texel, round_half_up((256 - F) * slice / 256).
+// a_fast tells whether axis a is the faster axis of the pair (rules 1, 2).
+struct W4 {
+    float w00, w01, w10, w11;
+};
+
+__device__ __forceinline__ float round_half_up(float x) { return floorf(x + 0.5f); }
+
+template <bool TEX8>
+__device__ __forceinline__ W4 weights4(float wa, float wb, int rule, bool a_fast) {
+    W4 w;
+    if (!TEX8) {
+        w.w00 = (1.f - wa) * (1.f - wb);
+        w.w01 = (1.f - wa) * wb;
+        w.w10 = wa * (1.f - wb);
+        w.w11 = wa * wb;
+        return w;
+    }
+    // integer arithmetic in float: every product is below 2^16, exact
+    if (rule == 0) {
+        w.w11 = round_half_up(wa * wb * (1.f / 256.f));
+        w.w10 = wa - w.w11;
+        w.w01 = wb - w.w11;
+        w.w00 = 256.f - wa - wb + w.w11;
+        return w;
+    }
+    const float F = a_fast ? wa : wb;
+    const float S = a_fast ? wb : wa;
+    const float G = rule == 1 ? F : 256.f - F;
+    const float x1 = round_half_up(G * S * (1.f / 256.f));          // anchor, slow 1
+    const float x0 = round_half_up(G * (256.f - S) * (1.f / 256.f));  // anchor, slow 0
+    const float y1 = S - x1, y0 = (256.f - S) - x0;
+    // fast-1 / fast-0 columns
+    const float f1s0 = rule == 1 ? x0 : y0, f1s1 = rule == 1 ? x1 : y1;
+    const float f0s0 = rule == 1 ? y0 : x0, f0s1 = rule == 1 ? y1 : x1;
+    if (a_fast) {
+        w.w00 = f0s0;
+        w.w01 = f0s1;
+        w.w10 = f1s0;
+        w.w11 = f1s1;
+    } else {
+        w.w00 = f0s0;
+        w.w01 = f1s0;
+        w.w10 = f0s1;
+        w.w11 = f1s1;
+    }
+    return w;
+}
+
+template <bool TEX8>
+__device__ __forceinline__ float combine4(float t00, float t01, float t10, float t11, const W4& w) {
+    if (TEX8) {
+        const float s = fmaf(w.w11, t11, fmaf(w.w10, t10, fmaf(w.w01, t01, __fmul_rn(w.w00, t00))));
+        return __fmul_rn(s, 1.f / 256.f);
+    }
+    return fmaf(w.w11, t11, fmaf(w.w10, t10, fmaf(w.w01, t01, __fmul_rn(w.w00, t00))));
+}
+
+// Bilinear fetch from a 2D plane with border zeros. c1 indexes the plane's
+// first axis (stride s1, n1 texels), c2 the second; rule/a_fast as for
+// weights4.
+template <bool TEX8, typename T>
+__device__ __forceinline__ float bilinear(const T* __restrict__ base, int64_t s1, int64_t s2, int n1,
+                                          int n2, float c1, float c2, int rule = 0, bool a_fast = true) {
+    const Split a = split_coord<TEX8>(c1);
+    const Split b = split_coord<TEX8>(c2);
+    const bool i0 = (unsigned)a.i < (unsigned)n1;
+    const bool i1 = (unsigned)(a.i + 1) < (unsigned)n1;
+    const bool j0 = (unsigned)b.i < (unsigned)n2;
+    const bool j1 = (unsigned)(b.i + 1) < (unsigned)n2;
+    const T* p = base + (int64_t)a.i * s1 + (int64_t)b.i * s2;
+    const float t00 = (i0 && j0) ? ld(p) : 0.f;
+    const float t01 = (i0 && j1) ? ld(p + s2) : 0.f;
+    const float t10 = (i1 && j0) ? ld(p + s1) : 0.f;
+    const float t11 = (i1 && j1) ? ld(p + s1 + s2) : 0.f;
+    return combine4<TEX8>(t00, t01, t10, t11, weights4<TEX8>(a.w, b.w, rule, a_fast));
+}
+
+}  // namespace kk
+
+// ---------------------------------------------------------------------------
+// host-side error reporting (kk_capi.cu)
+// ---------------------------------------------------------------------------
+int kk_fail(int status, const char* fmt, ...);
+int kk_check_launch(const char* what);

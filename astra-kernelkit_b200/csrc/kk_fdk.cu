@@ -1,0 +1,128 @@
+// FDK pre-processing kernels: cone-beam cosine pre-weighting and detector
+// row filtering, both in float64 as the reference evaluates them
+// (processing.py:96-126, 149-188), plus the SIRT reciprocal helper.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "kk_common.cuh"
+
+namespace kk {
+
+constexpr int PW_BLOCK = 256;
+constexpr int FILT_BLOCK = 256;
+constexpr int FILT_MAX_COLS = 8192;
+
+// p *= |d - s| / |pixel - s|; pixel = corner + col * u_pw + row * v_ph.
+// Evaluated with the operation order of processing.py:182-186 and of
+// numpy's norm (((dx*dx + dy*dy) + dz*dz), then sqrt), no fused
+// operations, then rounded once to float32 as the in-place float32
+// multiply of the reference does.
+__global__ void __launch_bounds__(PW_BLOCK)
+    preweight_kernel(float* data, const uint64_t* table, int64_t sa, int64_t sr, int64_t sc, int rows, int cols,
+                     const double* __restrict__ geom) {
+    const int a = blockIdx.y;
+    const int64_t pix = (int64_t)blockIdx.x * PW_BLOCK + threadIdx.x;
+    if (pix >= (int64_t)rows * cols) return;
+    const int r = (int)(pix / cols), c = (int)(pix % cols);
+    const double* g = geom + 13 * (int64_t)a;
+    double sq = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double p = __dadd_rn(__dadd_rn(g[k], __dmul_rn((double)c, g[3 + k])), __dmul_rn((double)r, g[6 + k]));
+        const double d = __dsub_rn(p, g[9 + k]);
+        sq = k == 0 ? __dmul_rn(d, d) : __dadd_rn(sq, __dmul_rn(d, d));
+    }
+    const double w = __ddiv_rn(g[12], __dsqrt_rn(sq));
+    float* e = (table ? (float*)table[a] : data + (int64_t)a * sa) + (int64_t)r * sr + (int64_t)c * sc;
+    *e = __double2float_rn(__dmul_rn((double)*e, w));
+}
+
+// out[i] = sum_j p[j] * h[(i - j) mod P] for one detector row; the row is
+// staged in shared memory as float64, h is read through the read-only
+// cache.
+__global__ void __launch_bounds__(FILT_BLOCK)
+    filter_rows_kernel(float* data, const uint64_t* table, int64_t sa, int64_t sr, int64_t sc, int rows, int cols,
+                       const double* __restrict__ h, int P) {
+    extern __shared__ double row[];
+    const int line = blockIdx.x;
+    const int a = line / rows, r = line % rows;
+    float* base = (table ? (float*)table[a] : data + (int64_t)a * sa) + (int64_t)r * sr;
+    for (int j = threadIdx.x; j < cols; j += FILT_BLOCK) row[j] = (double)base[(int64_t)j * sc];
+    __syncthreads();
+    for (int i = threadIdx.x; i < cols; i += FILT_BLOCK) {
+        double acc = 0.0;
+        for (int j = 0; j < cols; ++j) {
+            int k = i - j;
+            k += (k < 0) ? P : 0;
+            acc = fma(row[j], __ldg(h + k), acc);
+        }
+        base[(int64_t)i * sc] = __double2float_rn(acc);
+    }
+}
+
+__global__ void reciprocal_kernel(float* x, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float v = __fdiv_rn(1.f, x[i]);
+        x[i] = (v == __int_as_float(0x7f800000)) ? 0.f : v;
+    }
+}
+
+}  // namespace kk
+
+using namespace kk;
+
+static int check_f32_projections(const kk_projections* p, const char* who) {
+    if (!p || (!p->data && !p->table)) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: projections are NULL", who);
+    if (p->dtype != KK_F32) return kk_fail(KK_ERR_UNSUPPORTED, "%s: float32 projections only", who);
+    if (p->table && p->table_axis != 0)
+        return kk_fail(KK_ERR_UNSUPPORTED, "%s: a pointer table is supported along the angle axis only", who);
+    if (p->n_angles <= 0 || p->rows <= 0 || p->cols <= 0 || p->n_angles > 65535 || p->rows > (1 << 20) ||
+        p->cols > (1 << 20))
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: bad projection shape", who);
+    return KK_OK;
+}
+
+extern "C" int kk_preweight(const kk_projections* proj, const double* geom, void* stream) {
+    int rc = check_f32_projections(proj, "kk_preweight");
+    if (rc) return rc;
+    if (!geom) return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_preweight: geometry is NULL");
+    const int64_t npix = proj->rows * proj->cols;
+    dim3 grid((unsigned)((npix + PW_BLOCK - 1) / PW_BLOCK), (unsigned)proj->n_angles);
+    preweight_kernel<<<grid, PW_BLOCK, 0, (cudaStream_t)stream>>>(
+        (float*)proj->data, proj->table, proj->stride[0], proj->stride[1], proj->stride[2], (int)proj->rows,
+        (int)proj->cols, geom);
+    return kk_check_launch("kk_preweight");
+}
+
+extern "C" int kk_filter_rows(const kk_projections* proj, const double* h, int64_t P, void* stream) {
+    int rc = check_f32_projections(proj, "kk_filter_rows");
+    if (rc) return rc;
+    if (!h) return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_filter_rows: filter is NULL");
+    if (proj->cols > FILT_MAX_COLS)
+        return kk_fail(KK_ERR_UNSUPPORTED, "kk_filter_rows: at most %d columns", FILT_MAX_COLS);
+    if (P < 2 * proj->cols)
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_filter_rows: padded length %lld shorter than 2*cols",
+                       (long long)P);
+    const int64_t lines = proj->n_angles * proj->rows;
+    if (lines > 0x7fffffff) return kk_fail(KK_ERR_UNSUPPORTED, "kk_filter_rows: too many rows");
+    const size_t smem = sizeof(double) * (size_t)proj->cols;
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(filter_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(double) * FILT_MAX_COLS));
+        attr_set = true;
+    }
+    filter_rows_kernel<<<(unsigned)lines, FILT_BLOCK, smem, (cudaStream_t)stream>>>(
+        (float*)proj->data, proj->table, proj->stride[0], proj->stride[1], proj->stride[2], (int)proj->rows,
+        (int)proj->cols, h, (int)P);
+    return kk_check_launch("kk_filter_rows");
+}
+
+extern "C" int kk_reciprocal(float* data, int64_t n, void* stream) {
+    if (!data || n < 0) return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_reciprocal: bad arguments");
+    if (n == 0) return KK_OK;
+    int64_t blocks = (n + 255) / 256;
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    reciprocal_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(data, n);
+    return kk_check_launch("kk_reciprocal");
+}

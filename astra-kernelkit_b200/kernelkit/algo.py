@@ -1,0 +1,250 @@
+"""Reconstruction algorithms: forward/back projection helpers, FDK and SIRT.
+
+Mirrors ``kernelkit/algo.py`` of the reference (signatures, defaults and
+return conventions: host NumPy arrays unless device output is requested).
+SIRT runs two fused kernels per iteration, ``(A x - y) R`` in the forward
+projection's epilogue and ``x = clip(mask (x - C A^T r))`` in the
+backprojection's, and replays them from a CUDA graph when no per-iteration
+host work is requested.
+"""
+from __future__ import annotations
+
+from typing import Any, Callable, Sequence
+
+import numpy as np
+
+from . import _arrays, _native
+from .geom.proj import Beam, ProjectionGeometrySequence
+from .geom.vol import VolumeGeometry
+from .kernel import BaseKernel
+from .kernels.cone_bp import VoxelDrivenConeBP
+from .kernels.cone_fp import RayDrivenConeFP
+from .operator import XrayTransform
+from .processing import filter as filt
+from .processing import preweight
+from .projector import BackProjector
+
+
+def _to_host(dev, out=None):
+    host = dev.cpu().numpy() if out is None else None
+    if out is None:
+        return host
+    if isinstance(out, np.ndarray):
+        out[...] = dev.cpu().numpy()
+        return out
+    return out
+
+
+def fp(volume: Any, projection_geometry, volume_geometry: VolumeGeometry,
+       out=None):
+    """X-ray forward projection (``algo.py:18-49``). Returns a host array
+    unless ``out`` is a device array, which is then filled and returned."""
+    t = _arrays.torch()
+    op = XrayTransform(projection_geometry, volume_geometry)
+    vol = _arrays.as_tensor(volume, dtype=t.float32)
+    dev_out = out if (out is not None and _arrays.is_device_array(out)) \
+        else None
+    result = op(vol, out=_arrays.as_tensor(dev_out) if dev_out is not None
+                else None)
+    if dev_out is not None:
+        return out
+    return _to_host(result, out)
+
+
+def bp(projections: Any, projection_geometry, volume_geometry: VolumeGeometry,
+       filter: Any = None, preproc_fn: Callable = None,
+       kernel: BaseKernel = None, out=None,
+       projection_axes: Sequence[int] = (0, 1, 2), **kwargs):
+    """X-ray backprojection, optionally with FDK pre-weighting and
+    filtering (``algo.py:52-126``). Device float32 projections are
+    pre-processed in place, as in the reference. Returns a host array (or
+    fills a host ``out``)."""
+    t = _arrays.torch()
+    if out is not None and _arrays.is_device_array(out):
+        out_gpu = _arrays.as_tensor(out, dtype=t.float32)
+    else:
+        out_gpu = t.zeros(tuple(int(s) for s in volume_geometry.shape),
+                          dtype=t.float32, device="cuda")
+    projections = _arrays.as_tensor(projections, dtype=t.float32)
+    if preproc_fn is not None:
+        preproc_fn(projections, projection_geometry)
+    if filter is not None:
+        if tuple(projection_axes) != (0, 1, 2):
+            raise NotImplementedError()
+        preweight(projections, projection_geometry)
+        filt(projections, filter=filter)
+    kwargs.pop("beam", None)
+    kwargs.update(projection_axes=projection_axes)
+    ptor = BackProjector(VoxelDrivenConeBP(**kwargs) if kernel is None
+                         else kernel, texture_type="layered")
+    ptor.projection_geometry = projection_geometry
+    ptor.volume_geometry = volume_geometry
+    ptor.projections = projections
+    ptor.volume = out_gpu
+    ptor()
+    if isinstance(out, np.ndarray):
+        out[...] = out_gpu.cpu().numpy()
+        return out
+    return out_gpu.cpu().numpy()
+
+
+def fbp(projections: Any, projection_geometry, volume_geometry,
+        filter: Any = "ramlak", **bp_kwargs):
+    """Parallel-beam FBP is not implemented (as in the reference,
+    ``algo.py:129-166``)."""
+    raise NotImplementedError(
+        "FBP is not implemented yet. Use a conebeam geometry with the `bp` "
+        "function, or file an issue.")
+
+
+def fdk(projections: Any, projection_geometry: Any,
+        volume_geometry: VolumeGeometry, filter: Any = "ramlak", **bp_kwargs):
+    """Feldkamp-Davis-Kress reconstruction (``algo.py:169-223``):
+    pre-weighting, row filtering, then backprojection with the adjoint
+    scaling of ``VoxelDrivenConeBP``. No extra angular normalisation is
+    applied, exactly as in the reference."""
+    beams = ([projection_geometry.beam]
+             if isinstance(projection_geometry, ProjectionGeometrySequence)
+             else [p.beam for p in projection_geometry])
+    if any(b != Beam.CONE for b in beams):
+        raise NotImplementedError(
+            "Only cone beam geometry is supported at the moment.")
+    if "kernel" not in bp_kwargs:
+        bp_kwargs.update(kernel=VoxelDrivenConeBP())
+    return bp(projections, projection_geometry, volume_geometry,
+              filter=filter, **bp_kwargs)
+
+
+class SIRT:
+    """Reusable SIRT solver state (device buffers, kernel parameters and an
+    optional captured CUDA graph of one iteration).
+
+    ``x <- clip(mask * (x - C * A^T (R * (A x - y))))`` with
+    ``C = 1 / A^T 1`` and ``R = 1 / A 1`` (``+inf -> 0``), ``x_0 = 0``
+    (``algo.py:226-368``)."""
+
+    def __init__(self, projections, projection_geometry,
+                 volume_geometry: VolumeGeometry, mask=None,
+                 min_constraint: float = None, max_constraint: float = None,
+                 interpolation: str = "texture"):
+        t = _arrays.torch()
+        if len(projections) != len(projection_geometry):
+            raise ValueError(
+                "Number of projections does not match number of geometries.")
+        self.vg = volume_geometry
+        self.pg = projection_geometry
+        self.y = _arrays.as_tensor(projections, dtype=t.float32).contiguous()
+        if self.y.dim() != 3:
+            raise ValueError("Projections must be (angles, rows, cols).")
+        shape = tuple(int(s) for s in volume_geometry.shape)
+        self.fp = RayDrivenConeFP(interpolation=interpolation)
+        self.fp.compile()
+        self.fp.set_params(self.fp.geoms2params(projection_geometry,
+                                                volume_geometry))
+        self.bp = VoxelDrivenConeBP(interpolation=interpolation)
+        self.bp.compile()
+        self.bp.set_params(self.bp.geoms2params(projection_geometry,
+                                                volume_geometry))
+        self.x = t.zeros(shape, dtype=t.float32, device="cuda")
+        self.mask = (None if mask is None
+                     else _arrays.as_tensor(mask, dtype=t.float32).contiguous())
+        self.min_c, self.max_c = min_constraint, max_constraint
+        L = _native.load()
+        stream = _native.current_stream()
+        # C = 1 / A^T 1
+        self.C = t.empty(shape, dtype=t.float32, device="cuda")
+        ones = t.ones_like(self.y)
+        self.bp(ones, self.C, volume_geometry, additive=False)
+        _native.check(L.kk_reciprocal(self.C.data_ptr(), self.C.numel(),
+                                      stream))
+        del ones
+        # R = 1 / A 1
+        self.R = t.empty_like(self.y)
+        ones = t.ones(shape, dtype=t.float32, device="cuda")
+        self.fp(ones, self.pg, volume_geometry, self.R, additive=False)
+        _native.check(L.kk_reciprocal(self.R.data_ptr(), self.R.numel(),
+                                      stream))
+        del ones
+        self.y_tmp = t.empty_like(self.y)
+        self._graph = None
+
+    def step(self):
+        """One iteration: two kernel launches."""
+        self.fp.residual(self.x, self.pg, self.vg, self.y_tmp, self.y, self.R)
+        self.bp.update(self.y_tmp, self.x, self.vg, self.C, self.mask,
+                       self.min_c, self.max_c)
+
+    def capture(self):
+        """Capture one iteration into a CUDA graph (no work runs)."""
+        t = _arrays.torch()
+        g = t.cuda.CUDAGraph()
+        s = t.cuda.Stream()
+        s.wait_stream(t.cuda.current_stream())
+        with t.cuda.stream(s):
+            with t.cuda.graph(g, stream=s):
+                self.step()
+        t.cuda.current_stream().wait_stream(s)
+        self._graph = g
+        return g
+
+    def run(self, iters: int, use_graph: bool = True, callback=None,
+            progress=None):
+        for i in range(iters):
+            if use_graph:
+                if self._graph is None:
+                    self.capture()
+                self._graph.replay()
+            else:
+                self.step()
+            if progress is not None:
+                progress(i)
+            if callback is not None:
+                callback(i, self.x, self.y_tmp)
+        return self.x
+
+
+def sirt(projections: np.ndarray, projection_geometry: Any,
+         volume_geometry: VolumeGeometry, iters: int = 100,
+         verbose: bool = True, mask: Any = None,
+         min_constraint: float = None, max_constraint: float = None,
+         return_gpu: bool = False, callback: callable = None,
+         residual_every: int = 10, use_graph: bool | None = None):
+    """Simultaneous Iterative Reconstruction Technique (``algo.py:226-368``).
+
+    Projections are (angles, rows, cols). Returns the volume as a host
+    array, or as a device tensor with ``return_gpu``. ``callback(i, x,
+    residual)`` runs after each iteration. The iteration is replayed from a
+    CUDA graph unless a callback or the verbose residual display needs the
+    host between iterations (``use_graph`` overrides)."""
+    solver = SIRT(projections, projection_geometry, volume_geometry,
+                  mask=mask, min_constraint=min_constraint,
+                  max_constraint=max_constraint)
+    show = verbose and residual_every is not None
+    if use_graph is None:
+        use_graph = callback is None and not show
+    progress = None
+    bar = None
+    if verbose:
+        from tqdm import tqdm
+
+        bar = tqdm(total=iters, desc="SIRT")
+        state = {"norm": ""}
+
+        def progress(i):
+            if show:
+                E = residual_every
+                if i % E == 0:
+                    state["norm"] = str(float(solver.y_tmp.norm()))
+                desc = "SIRT [" + "*" * (i % E) + "." * (E - i % E) + "]"
+                bar.set_description(f"{desc}: {state['norm']})")
+            bar.update(1)
+    x = solver.run(iters, use_graph=use_graph, callback=callback,
+                   progress=progress)
+    if bar is not None:
+        bar.close()
+    if return_gpu:
+        return x
+    return x.cpu().numpy()
+
+
+__all__ = ["fp", "bp", "fbp", "fdk", "sirt", "SIRT"]

@@ -1,0 +1,339 @@
+"""Ray-driven cone-beam forward projection kernel.
+
+Python face of ``kk_cone_fp`` (``include/kk.h``), mirroring
+``kernelkit/kernels/cone_fp.py`` of the reference: same class name,
+constructor options, ``compile``/``geoms2params``/``set_params``/
+``__call__`` protocol and exceptions. Per-angle parameters live in device
+memory owned by the kernel object (the reference uses ``__constant__``
+memory capped at ``max_projs`` angles; here there is no cap).
+"""
+from __future__ import annotations
+
+import copy
+from typing import Sequence
+
+import numpy as np
+
+from .. import _arrays, _native
+from ..geom import normalize_
+from ..geom.proj import ProjectionGeometrySequence
+from ..geom.vol import VolumeGeometry
+from ..kernel import (BaseKernel, KernelMemoryUnpreparedException,
+                      KernelNotCompiledException, Texture)
+
+_INTERP = {"texture": _native.KK_INTERP_TEX8, "tex8": _native.KK_INTERP_TEX8,
+           "exact": _native.KK_INTERP_EXACT, "linear": _native.KK_INTERP_EXACT}
+
+
+def interp_code(name: str) -> int:
+    try:
+        return _INTERP[name.lower()]
+    except KeyError:
+        raise ValueError(
+            f"`interpolation` must be one of {sorted(_INTERP)}, got {name!r}.")
+
+
+class ConeFPParams(tuple):
+    """The 12 float32 parameter arrays of ``geoms2params`` (source xyz,
+    detector corner xyz, u*pixel_width xyz, v*pixel_height xyz; reference
+    ``kernels/cone_fp.py:330-339``) plus ``axes``, the dominant ray axis
+    per angle (``kernels/cone_fp.py:264-285``)."""
+
+    axes: np.ndarray | None
+
+    def __new__(cls, arrays, axes=None):
+        obj = super().__new__(cls, arrays)
+        obj.axes = axes
+        return obj
+
+
+#: device pointer tables of recently used projection lists, so repeated
+#: calls on the same list upload nothing (and can be graph-captured)
+_TABLES: dict = {}
+
+
+def list_desc(projections, projection_axes):
+    """Descriptor (and keep-alive objects) of a list of 2D per-angle device
+    arrays, e.g. pitched views from ``kernelkit.aspitched``; entry axes are
+    the logical axes ``projection_axes[1:]``. All entries must share one
+    layout."""
+    t = _arrays.torch()
+    if projection_axes[0] != 0:
+        raise ValueError(
+            "A list of projections requires projection_axes[0] == 0.")
+    arrs = [_arrays.as_tensor(p) for p in projections]
+    if len(arrs) == 0:
+        raise ValueError("Empty list of projections.")
+    first = arrs[0]
+    for a in arrs:
+        if a.dim() != 2:
+            raise ValueError("Projection list entries must be 2D.")
+        if (a.shape != first.shape or a.stride() != first.stride()
+                or a.dtype != first.dtype):
+            raise ValueError("Projection list entries must share shape, "
+                             "strides and dtype.")
+    r_ax = projection_axes.index(1) - 1
+    c_ax = projection_axes.index(2) - 1
+    key = tuple(a.data_ptr() for a in arrs)
+    table = _TABLES.pop(key, None)
+    if table is None:
+        table = t.tensor(key, dtype=t.int64, device="cuda")
+    _TABLES[key] = table  # most recent last
+    while len(_TABLES) > 8:
+        _TABLES.pop(next(iter(_TABLES)))
+    d = _native.table_desc(table, len(arrs), first.shape[r_ax],
+                           first.shape[c_ax], first.stride(r_ax),
+                           first.stride(c_ax), _native.dtype_code(first))
+    return d, (arrs, table)
+
+
+def _sequence(projection_geometry) -> ProjectionGeometrySequence:
+    if isinstance(projection_geometry, ProjectionGeometrySequence):
+        return copy.deepcopy(projection_geometry)
+    return ProjectionGeometrySequence.fromList(projection_geometry)
+
+
+class RayDrivenConeFP(BaseKernel):
+    """Ray-driven (Joseph) cone-beam forward projection.
+
+    Every ray steps one slice at a time along its dominant world axis and
+    sums bilinear samples of the volume at the slice centres, times the
+    distance correction; ``interpolation='texture'`` (default) samples with
+    the texture unit's 1/256 weights as the reference does,
+    ``'exact'`` with exact weights.
+    """
+
+    FLOAT_DTYPE = np.float32
+    SUPPORTED_DTYPES = ("float32", "bfloat16", "float16")
+
+    pixels_per_block = (1, 32, 32)
+    slices_per_block = 16
+
+    def __init__(self, pixels_per_block: tuple = None,
+                 slices_per_block: int = None,
+                 volume_axes: tuple = (0, 1, 2),
+                 projection_axes: tuple = (0, 1, 2),
+                 interpolation: str = "texture"):
+        super().__init__()
+        if pixels_per_block is not None:
+            self.pixels_per_block = tuple(pixels_per_block)
+        if slices_per_block is not None:
+            if int(slices_per_block) <= 0:
+                raise ValueError("`slices_per_block` must be positive.")
+            self.slices_per_block = int(slices_per_block)
+        for name, axes in (("volume_axes", volume_axes),
+                           ("projection_axes", projection_axes)):
+            if sorted(axes) != [0, 1, 2]:
+                raise ValueError(f"`{name}` must be a permutation of "
+                                 f"(0, 1, 2), got {axes}.")
+        self._vol_axs = tuple(volume_axes)
+        self._proj_axs = tuple(projection_axes)
+        self._interp = interp_code(interpolation)
+        self.interpolation = interpolation
+        self._params_dev = None
+        self._n_params = 0
+        self._axes_known = False
+
+    @property
+    def volume_axes(self) -> tuple:
+        return self._vol_axs
+
+    @property
+    def projection_axes(self) -> tuple:
+        return self._proj_axs
+
+    @property
+    def _params_are_set(self) -> bool:
+        return self._params_dev is not None
+
+    def compile(self, max_projs: int = 1024):
+        """Validate options and load the native library. ``max_projs`` is
+        accepted for compatibility; there is no per-kernel angle cap."""
+        return self._compile(dict(
+            slices_per_block=self.slices_per_block,
+            rows_per_block=self.pixels_per_block[1],
+            cols_per_block=self.pixels_per_block[2],
+            nr_projs_global=int(max_projs),
+            volume_axes=self._vol_axs, projection_axes=self._proj_axs,
+            interpolation=self.interpolation))
+
+    # -- parameters ---------------------------------------------------------
+    @staticmethod
+    def _geom_axes(projection_geometry) -> np.ndarray:
+        """Dominant world axis of each ray (argmax |source - detector|)."""
+        pg = projection_geometry
+        return np.argmax(np.abs(pg.source_position - pg.detector_position),
+                         axis=1)
+
+    @staticmethod
+    def _output_scale(voxel_size) -> list:
+        """(scale1, scale2, outputScale) per dominant axis
+        (``kernels/cone_fp.py:287-300``)."""
+        eps = 1e-4
+        v = voxel_size
+        if abs(v[0] / v[1] - 1) > eps or abs(v[0] / v[2] - 1) > eps:
+            x = [(v[1] / v[0]) ** 2, (v[2] / v[0]) ** 2, v[0] ** 2]
+            y = [(v[0] / v[1]) ** 2, (v[2] / v[1]) ** 2, v[0] * v[1]]
+            z = [(v[0] / v[2]) ** 2, (v[1] / v[2]) ** 2, v[0] * v[2]]
+            return [x, y, z]
+        return [[1.0, 1.0, v[0]]] * 3
+
+    @staticmethod
+    def geoms2params(projection_geometry, volume_geometry: VolumeGeometry
+                     ) -> ConeFPParams:
+        """Kernel parameters in the volume's unit-voxel frame.
+
+        Same float32 values as the reference (``kernels/cone_fp.py:
+        302-339``) but computed on a copy: the caller's geometry is not
+        normalised in place."""
+        pg = _sequence(projection_geometry)
+        normalize_(pg, volume_geometry)
+        src = np.ascontiguousarray(pg.source_position.T)
+        corner = np.ascontiguousarray(pg.detector_extent_min.T)
+        u = np.ascontiguousarray(pg.u.T * pg.detector.pixel_width)
+        v = np.ascontiguousarray(pg.v.T * pg.detector.pixel_height)
+        arrays = (src[0], src[1], src[2], corner[0], corner[1], corner[2],
+                  u[0], u[1], u[2], v[0], v[1], v[2])
+        return ConeFPParams(arrays, RayDrivenConeFP._geom_axes(pg))
+
+    def set_params(self, params):
+        """Upload the per-angle parameters to the device."""
+        if not self.is_compiled:
+            raise KernelNotCompiledException(
+                f"Compile {self.__class__.__name__} before setting its "
+                "parameters.")
+        if len(params) != 12 or any(len(p) != len(params[0]) for p in params):
+            raise ValueError("Expected 12 equally long parameter arrays.")
+        n = len(params[0])
+        rec = np.zeros(n, _native.FP_ANGLE_DTYPE)
+        stack = np.stack([np.asarray(p, np.float32) for p in params], axis=1)
+        rec["src"] = stack[:, 0:3]
+        rec["corner"] = stack[:, 3:6]
+        rec["u"] = stack[:, 6:9]
+        rec["v"] = stack[:, 9:12]
+        axes = getattr(params, "axes", None)
+        self._axes_known = axes is not None
+        rec["axis"] = axes if axes is not None else 0
+        self._host_params = rec
+        t = _arrays.torch()
+        self._params_dev = t.from_numpy(rec.view(np.uint8)).cuda()
+        self._n_params = n
+
+    def _ensure_axes(self, projection_geometry, volume_geometry):
+        if self._axes_known:
+            return
+        pg = _sequence(projection_geometry)
+        normalize_(pg, volume_geometry)
+        self._host_params["axis"] = self._geom_axes(pg)
+        t = _arrays.torch()
+        self._params_dev = t.from_numpy(self._host_params.view(np.uint8)
+                                        ).cuda()
+        self._axes_known = True
+
+    # -- launch -------------------------------------------------------------
+    def _output(self, projections, projection_geometry, projections_pitch):
+        """(descriptor, keep-alive objects) for the projections argument."""
+        t = _arrays.torch()
+        if isinstance(projections, (list, tuple)):
+            if self._proj_axs[0] != 0:
+                raise ValueError(
+                    "A list of projections requires projection_axes[0] == 0.")
+            return list_desc(projections, self._proj_axs)
+        arr = _arrays.as_tensor(projections)
+        if arr.dtype == t.int64 and arr.dim() == 1:
+            # the reference's low-level form: device table of per-angle
+            # pointers, optionally into pitched rows
+            if self._proj_axs[0] != 0:
+                raise NotImplementedError(
+                    "Pointer tables are supported along the angle axis only.")
+            rows = int(projection_geometry.detector.rows[0])
+            cols = int(projection_geometry.detector.cols[0])
+            pitch = projections_pitch or (len(arr), rows, cols)
+            if self._proj_axs == (0, 1, 2):
+                rs, cs = pitch[2], 1
+            else:
+                rs, cs = 1, pitch[1]
+            d = _native.table_desc(arr, len(arr), rows, cols, rs, cs,
+                                   _native.KK_F32)
+            return d, (arr,)
+        return _native.projections_desc(arr, self._proj_axs), (arr,)
+
+    def __call__(self, volume_texture, projection_geometry,
+                 volume_geometry: VolumeGeometry, projections,
+                 projections_pitch: tuple | None = None,
+                 additive: bool = True):
+        """Project ``volume_texture`` into ``projections``.
+
+        As in the reference the result is added to ``projections``; pass
+        ``additive=False`` to overwrite instead (saves zero-filling).
+        ``volume_texture`` is a ``Texture`` from ``copy_to_texture`` or a
+        device array laid out by ``volume_axes``; ``projections`` a device
+        array laid out by ``projection_axes``, a list of 2D device arrays,
+        or an int64 device array of per-angle pointers."""
+        if volume_texture is None:
+            raise ValueError("`volume_texture` is None.")
+        if not self.is_compiled:
+            raise KernelNotCompiledException(
+                "Please compile the kernel with `compile()`.")
+        if not self._params_are_set:
+            raise KernelMemoryUnpreparedException(
+                "Please set the projection geometry with `set_params()`.")
+        if not isinstance(projection_geometry, ProjectionGeometrySequence):
+            projection_geometry = ProjectionGeometrySequence.fromList(
+                projection_geometry)
+        if len(projection_geometry) != self._n_params:
+            raise ValueError(
+                f"Parameters were set for {self._n_params} angles, but the "
+                f"geometry has {len(projection_geometry)}.")
+        self._ensure_axes(projection_geometry, volume_geometry)
+        vol = (volume_texture.array if isinstance(volume_texture, Texture)
+               else _arrays.as_tensor(volume_texture))
+        vdesc = _native.volume_desc(vol, self._vol_axs)
+        expect = tuple(int(s) for s in volume_geometry.shape)
+        if tuple(vdesc.shape) != expect:
+            raise ValueError(
+                f"Volume of world shape {tuple(vdesc.shape)} does not match "
+                f"the volume geometry {expect}.")
+        pdesc, keep = self._output(projections, projection_geometry,
+                                   projections_pitch)
+        if pdesc.n_angles != self._n_params:
+            raise ValueError(
+                f"{pdesc.n_angles} projections given for {self._n_params} "
+                "angles.")
+        det = projection_geometry.detector
+        if (pdesc.rows, pdesc.cols) != (int(det.rows[0]), int(det.cols[0])):
+            raise ValueError(
+                f"Projections of {pdesc.rows}x{pdesc.cols} pixels do not "
+                f"match the detector {int(det.rows[0])}x{int(det.cols[0])}.")
+        osc = np.asarray(self._output_scale(volume_geometry.voxel_size),
+                         np.float32).reshape(9)
+        L = _native.load()
+        _native.check(L.kk_cone_fp(
+            vdesc, pdesc, self._params_dev.data_ptr(), osc.ctypes.data,
+            self._interp, self.slices_per_block, int(bool(additive)),
+            _native.current_stream()))
+        del keep
+
+    def residual(self, volume, projection_geometry,
+                 volume_geometry: VolumeGeometry, out, measured, weight):
+        """Fused SIRT residual step: ``out = (A volume - measured) * weight``
+        (one kernel; reference ``algo.py:339-344``). All arrays are float32
+        device arrays in the ``projection_axes`` layout."""
+        if not self._params_are_set:
+            raise KernelMemoryUnpreparedException(
+                "Please set the projection geometry with `set_params()`.")
+        self._ensure_axes(projection_geometry, volume_geometry)
+        vdesc = _native.volume_desc(volume, self._vol_axs)
+        pdesc = _native.projections_desc(out, self._proj_axs)
+        for name, a in (("measured", measured), ("weight", weight)):
+            if a.shape != out.shape or a.stride() != out.stride():
+                raise ValueError(f"`{name}` must have the layout of `out`.")
+        res = _native.kk_fp_residual(measured.data_ptr(), weight.data_ptr())
+        osc = np.asarray(self._output_scale(volume_geometry.voxel_size),
+                         np.float32).reshape(9)
+        _native.check(_native.load().kk_cone_fp_residual(
+            vdesc, pdesc, self._params_dev.data_ptr(), osc.ctypes.data, res,
+            self._interp, self.slices_per_block, _native.current_stream()))
+
+
+__all__ = ["RayDrivenConeFP", "ConeFPParams"]

@@ -1,0 +1,178 @@
+/*
+ * kk.h - C ABI of the B200 cone-beam projection library (libkk.so).
+ *
+ * Drop-in boundary for the cone-beam hot path of ASTRA KernelKit. Every
+ * entry point takes plain device pointers, sizes and strides plus a CUDA
+ * stream (as void*), launches asynchronously on that stream, allocates no
+ * device memory, performs no host<->device copies and never synchronises,
+ * so calls may be captured in CUDA graphs. Each returns a kk_status;
+ * kk_last_error() describes the most recent failure of the calling thread.
+ *
+ * Coordinates follow the reference: volumes are indexed by world axes
+ * (x, y, z) with caller-given element strides (default layout vol[x][y][z],
+ * z fastest); projections by (angle, row, col) with caller-given strides or
+ * a per-index pointer table (list-of-arrays / pitched data).
+ */
+#ifndef KK_H
+#define KK_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KK_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define KK_API __attribute__((visibility("default")))
+#else
+#define KK_API
+#endif
+
+typedef enum {
+    KK_OK = 0,
+    KK_ERR_INVALID_ARGUMENT = 1,
+    KK_ERR_UNSUPPORTED = 2,
+    KK_ERR_CUDA = 3,
+    KK_ERR_TIMEOUT = 4
+} kk_status;
+
+typedef enum { KK_F32 = 0, KK_BF16 = 1, KK_F16 = 2 } kk_dtype;
+
+/* Interpolation weights. KK_INTERP_TEX8 reproduces the hardware texture
+ * filter the reference samples with (weights on a 1/256 grid) and is the
+ * reference-compatible default; KK_INTERP_EXACT uses exact float32
+ * weights. */
+typedef enum { KK_INTERP_TEX8 = 0, KK_INTERP_EXACT = 1 } kk_interp;
+
+/* Per-angle forward-projection parameters (device array, one per angle),
+ * in the normalised unit-voxel frame of the volume (reference:
+ * kernels/cone_fp.py:302-339 geoms2params, plus the dominant ray axis of
+ * kernels/cone_fp.py:264-285 _geom_axes). */
+typedef struct {
+    float src[3];      /* source position */
+    float corner[3];   /* detector corner (outer edge of pixel (0, 0)) */
+    float u[3];        /* column step: u * pixel_width */
+    float v[3];        /* row step: v * pixel_height */
+    int32_t axis;      /* dominant ray axis 0/1/2 (world x/y/z) */
+    int32_t pad[3];
+} kk_fp_angle;
+
+/* Per-angle backprojection parameters: the reference's Params struct
+ * (cuda/cone_bp.cu:27-33; kernels/cone_bp.py:304-421), each float4 stored
+ * as (x, y, z, w) = coefficients of world X, Y, Z and the constant. */
+typedef struct {
+    float num_u[4];
+    float num_v[4];
+    float den[4];
+} kk_bp_angle;
+
+typedef struct {
+    void* data;          /* device pointer to voxel (0, 0, 0) */
+    int64_t shape[3];    /* voxel counts along world x, y, z */
+    int64_t stride[3];   /* element strides along world x, y, z */
+    int32_t dtype;       /* kk_dtype */
+} kk_volume;
+
+typedef struct {
+    void* data;              /* device pointer to pixel (0, 0, 0); unused
+                                when table != NULL */
+    const uint64_t* table;   /* optional device array of base addresses
+                                indexed along table_axis */
+    int32_t table_axis;      /* 0 angle, 1 row, 2 col */
+    int64_t n_angles, rows, cols;
+    int64_t stride[3];       /* element strides for angle, row, col (the
+                                table axis' stride is ignored) */
+    int32_t dtype;           /* kk_dtype */
+} kk_projections;
+
+/* Optional fused epilogue of the forward projection (SIRT residual step,
+ * reference algo.py:339-344): out = (A x - y) * weight, elementwise in the
+ * layout of `out`. y and weight are float32 and share out's strides. */
+typedef struct {
+    const float* y;
+    const float* weight;
+} kk_fp_residual;
+
+/* Optional fused epilogue of the backprojection (SIRT update, reference
+ * algo.py:356-362): x = clip(mask * (x - scale * A^T r)), in place on the
+ * volume passed to kk_cone_bp_update. scale/mask are float32 with the
+ * volume's strides; mask may be NULL. */
+typedef struct {
+    const float* scale;
+    const float* mask;
+    float min_value;
+    float max_value;
+    int32_t has_min;
+    int32_t has_max;
+} kk_bp_update;
+
+/* ---- forward projection -------------------------------------------- */
+
+/* Ray-driven cone-beam forward projection (replaces the reference's
+ * RayDrivenConeFP.__call__, kernels/cone_fp.py:102-262, and its kernel
+ * cuda/cone_fp.cu:73-207). proj = A vol (additive=0) or proj += A vol.
+ * out_scale: host array of 9 floats, per dominant axis (scale1, scale2,
+ * outputScale) as kernels/cone_fp.py:287-300. slab: slices per coordinate
+ * restart, the reference's slices_per_block (16 by default; <= 0 selects
+ * 16). */
+KK_API int kk_cone_fp(const kk_volume* vol, const kk_projections* proj,
+                      const kk_fp_angle* angles, const float* out_scale,
+                      int32_t interp, int32_t slab, int32_t additive,
+                      void* stream);
+
+/* Forward projection with the SIRT residual epilogue (kk_fp_residual). */
+KK_API int kk_cone_fp_residual(const kk_volume* vol, const kk_projections* out,
+                               const kk_fp_angle* angles,
+                               const float* out_scale,
+                               const kk_fp_residual* residual, int32_t interp,
+                               int32_t slab, void* stream);
+
+/* ---- backprojection ------------------------------------------------- */
+
+/* Voxel-driven cone-beam backprojection (replaces VoxelDrivenConeBP.__call__,
+ * kernels/cone_bp.py:192-302, kernel cuda/cone_bp.cu:35-159).
+ * vol = A^T proj * out_scale (additive=0) or vol += ...; out_scale is the
+ * voxel volume (kernels/cone_bp.py:294). */
+KK_API int kk_cone_bp(const kk_projections* proj, const kk_volume* vol,
+               const kk_bp_angle* angles, float out_scale, int32_t interp,
+               int32_t additive, void* stream);
+
+/* Backprojection fused with the SIRT update epilogue (kk_bp_update). */
+KK_API int kk_cone_bp_update(const kk_projections* proj, const kk_volume* vol,
+                      const kk_bp_angle* angles, float out_scale,
+                      const kk_bp_update* update, int32_t interp,
+                      void* stream);
+
+/* ---- FDK pre-processing ---------------------------------------------- */
+
+/* Cone-beam cosine pre-weighting (replaces processing.preweight,
+ * processing.py:149-188): p *= |d - s| / |pixel - s| in float64, pixel at
+ * the pixel corner. geom: device array of 13 doubles per angle: corner[3],
+ * u*pw[3], v*ph[3], source[3], central ray length. */
+KK_API int kk_preweight(const kk_projections* proj, const double* geom,
+                 void* stream);
+
+/* Row filtering (replaces processing.filter, processing.py:96-126): every
+ * detector row p (length cols) becomes sum_j p[j] h[(i - j) mod P] in
+ * float64, h the real impulse response (length P) of the reference's
+ * frequency-domain filter. */
+KK_API int kk_filter_rows(const kk_projections* proj, const double* h, int64_t P,
+                   void* stream);
+
+/* ---- elementwise helpers -------------------------------------------- */
+
+/* x = 1 / x with +inf mapped to 0 (SIRT scaling, algo.py:320-333). */
+KK_API int kk_reciprocal(float* data, int64_t n, void* stream);
+
+/* ---- status ------------------------------------------------------- */
+
+KK_API const char* kk_last_error(void);
+KK_API int kk_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KK_H */
