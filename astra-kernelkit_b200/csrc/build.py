@@ -42,10 +42,11 @@ def stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(verbose: bool = False, force: bool = False, extra=()) -> str:
+def build(verbose: bool = False, force: bool = False, extra=(),
+          out: str = OUT) -> str:
     if not force and not stale():
-        return OUT
-    os.makedirs(os.path.dirname(OUT), exist_ok=True)
+        return out
+    os.makedirs(os.path.dirname(out), exist_ok=True)
     tmp = tempfile.mkdtemp(prefix="kk_build_")
     try:
         objs = []
@@ -60,10 +61,10 @@ def build(verbose: bool = False, force: bool = False, extra=()) -> str:
         lib = os.path.join(tmp, "libkk.so")
         subprocess.run([nvcc(), *ARCH, "-shared", *objs, "-o", lib,
                         "-lcudart"], check=True)
-        shutil.move(lib, OUT)
+        shutil.move(lib, out)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
-    return OUT
+    return out
 
 
 if __name__ == "__main__":

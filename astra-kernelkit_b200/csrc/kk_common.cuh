@@ -65,27 +65,31 @@ __device__ __forceinline__ void st<__half>(__half* p, float v) { *p = __float2ha
 // KK_INTERP_EXACT splits the float32 coordinate exactly and interpolates
 // separably.
 //
-// Coordinates are clamped to +-2^15 first: far outside any array every
+// Coordinates are clamped to +-2^14 first: far outside any array every
 // texel is a border zero either way, the clamp keeps the integer
-// conversion defined (non-finite values land on a border too), and below
-// 2^15 the half-up rounding x * 256 + 0.5 is exact. Arrays are therefore
-// limited to 32767 texels per axis (checked on the host).
-constexpr float COORD_LIMIT = 32768.f;
+// conversion defined (non-finite values land on a border too) and keeps
+// the fixed-point split below exact. Arrays are therefore limited to
+// 16383 texels per axis (checked on the host).
+constexpr float COORD_LIMIT = 16384.f;
 
 struct Split {
     int i;    // left texel
     float w;  // weight of texel i + 1: integer 0..255 (TEX8) or [0, 1)
 };
 
+// Split without the clamp, for coordinates known to lie within
+// +-COORD_LIMIT. TEX8: Q = floor(256 x + 1/2) - 128 is the half-up rounded
+// texel position in 1/256 units; adding 1.5 * 2^23 with round-down puts Q
+// in the low mantissa bits (exact for |Q| < 2^22), from which the index
+// (Q >> 8) and the weight (Q & 255) are read without conversions.
 template <bool TEX8>
-__device__ __forceinline__ Split split_coord(float x) {
-    x = fminf(fmaxf(x, -COORD_LIMIT), COORD_LIMIT);
+__device__ __forceinline__ Split split_unclamped(float x) {
     Split s;
     if (TEX8) {
-        const float q = floorf(x * 256.f + 0.5f) - 128.f;  // exact below 2^15
-        const float fi = floorf(q * (1.f / 256.f));
-        s.i = (int)fi;
-        s.w = q - fi * 256.f;
+        const float m = __fadd_rd(__fmaf_rd(x, 256.f, -127.5f), 12582912.f);
+        const int bits = __float_as_int(m);
+        s.i = (bits >> 8) - 0x4B4000;
+        s.w = __int_as_float((bits & 255) | 0x4B000000) - 8388608.f;
     } else {
         const float xb = x - 0.5f;
         const float fi = floorf(xb);
@@ -94,6 +98,16 @@ __device__ __forceinline__ Split split_coord(float x) {
     }
     return s;
 }
+
+template <bool TEX8>
+__device__ __forceinline__ Split split_coord(float x) {
+    return split_unclamped<TEX8>(fminf(fmaxf(x, -COORD_LIMIT), COORD_LIMIT));
+}
+
+// Scale of the weights returned by split_*: 256 for TEX8 (integer
+// weights), 1 otherwise.
+template <bool TEX8>
+__device__ __forceinline__ constexpr float weight_unit() { return TEX8 ? 256.f : 1.f; }
 
 // Weights of a bilinear footprint, indexed [a][b] by the left/right texel
 // along the two axes. For KK_INTERP_TEX8 they are the texture unit's

@@ -20,8 +20,6 @@
 namespace kk {
 
 constexpr int FP_SLAB = 16;       // default slices per coordinate restart
-constexpr int FP_TILE_R = 32;     // rays per block along detector rows (lanes)
-constexpr int FP_TILE_C = 8;      // rays per block along detector columns
 constexpr int BP_GROUP = 6;       // voxels per thread along the slowest axis
 constexpr int BP_CHUNK = 32;      // angles per accumulation chunk
 constexpr int BP_TILE_2 = 32;     // voxels per block along the fastest axis
@@ -39,14 +37,16 @@ struct FpArgs {
     const uint64_t* table;
     int64_t ps[3];
     int rows, cols;
-    int angle0;  // first angle of this launch
-    int slab;    // slices per coordinate restart
+    int n_angles;
+    int col_tiles;  // column tiles per angle
+    int slab;       // slices per coordinate restart
     const kk_fp_angle* angles;
     float os[9];
     const float* res_y;
     const float* res_w;
     int additive;
     int rank[3];  // memory rank of each world axis: 0 fastest .. 2 slowest
+    cudaTextureObject_t vtex;  // layered texture of the volume, or 0
 };
 
 struct BpArgs {
@@ -65,24 +65,151 @@ struct BpArgs {
     const float* upd_mask;
     float vmin, vmax;
     int has_min, has_max;
+    cudaTextureObject_t tex;  // layered texture of the projections (FETCH_TEX)
+    int j_begin, j_end;       // angles of this launch (one accumulation chunk)
+    int load_mode;            // running sum starts from 0 (LOAD_ZERO), vol, work
+    int store_mode;           // partial sum goes to vol (STORE_VOL) or work
+    float* work;              // float32 running sums between launches
 };
+
+enum BpLoad { LOAD_ZERO = 0, LOAD_VOL = 1, LOAD_WORK = 2 };
+enum BpStore { STORE_VOL = 0, STORE_WORK = 1, STORE_FINAL = 2 };
+
+enum BpFetch { FETCH_GLOBAL = 0, FETCH_TEX = 1 };
+
+}  // namespace kk
+
+// 2D-layered CUDA array with a linear-filtering, border-addressed texture
+struct kk_layered {
+    cudaArray_t array;
+    cudaTextureObject_t tex;
+    int64_t layers, height, width;
+    int32_t dtype;
+};
+
+namespace kk {
 
 __device__ __forceinline__ float pick3(const float* v, int k) {
     return k == 0 ? v[0] : (k == 1 ? v[1] : v[2]);
 }
 
 // ---------------------------------------------------------------------------
-// forward projection: one thread per ray, whole ray in 16-slice slabs
+// forward projection
 // ---------------------------------------------------------------------------
-template <typename TV, typename TP, bool TEX8, int EPI>
-__global__ void __launch_bounds__(FP_TILE_R* FP_TILE_C)
-    cone_fp_kernel(const FpArgs L) {
-    const int a = L.angle0 + blockIdx.y;
-    const int r = blockIdx.x % ((L.rows + FP_TILE_R - 1) / FP_TILE_R) * FP_TILE_R + threadIdx.x;
-    const int c = blockIdx.x / ((L.rows + FP_TILE_R - 1) / FP_TILE_R) * FP_TILE_C + threadIdx.y;
-    if (r >= L.rows || c >= L.cols) return;
+// Block = one angle, FP_COLS detector columns (one per warp) x FP_ROWS_T
+// rows; lane l of warp w traces rows r0 + l + 32 k (k < FP_RPT) of column
+// c0 + w, so a warp's loads for one slice cover consecutive rows, i.e.
+// consecutive positions along the fastest volume axis in the usual layout.
+// Blocks are ordered (row tile, angle, column tile) with the row tile
+// slowest: for circular scans about z the rows of a tile see one z-slab of
+// the volume, which then stays in L2 while every angle projects it.
+//
+// Three code paths, chosen per block: the ray's second in-slice axis D2 is
+// the unit-stride axis (FAST) and, in addition, the detector's v vector has
+// no component along the ray axis and D1 (SHARED): then every row of a
+// column sees the same D1 coordinate sequence, bit for bit, and the D1
+// split is done once per slice for the thread's rows. Otherwise a generic
+// per-ray path with arbitrary strides is used.
+#ifndef KK_FP_RPT
+#define KK_FP_RPT 2
+#endif
+#ifndef KK_FP_MINBLOCKS
+#define KK_FP_MINBLOCKS 5
+#endif
+constexpr int FP_RPT = KK_FP_RPT;       // rays per thread
+constexpr int FP_COLS = 8;              // columns per block (one per warp)
+constexpr int FP_ROWS_T = 32 * FP_RPT;  // rows per block
 
-    const kk_fp_angle* P = L.angles + a;
+struct RaySetup {
+    float a1, a2, b1, b2, corr;
+};
+
+// Per-ray slopes/offsets with the reference's float32 operation sequence
+// (cuda/cone_fp.cu:150-170, 197).
+__device__ __forceinline__ RaySetup ray_setup(const float* src, const float* cor, const float* u, const float* v,
+                                              int A, int D1, int D2, int r, int c, float sc1, float sc2) {
+    float det[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float ds = __fadd_rn(__fadd_rn(cor[k], __fmul_rn(0.5f, u[k])), __fmul_rn(0.5f, v[k]));
+        det[k] = fmaf((float)r, v[k], fmaf((float)c, u[k], ds));
+    }
+    RaySetup R;
+    const float sA = pick3(src, A), s1 = pick3(src, D1), s2 = pick3(src, D2);
+    const float sdd = __fsub_rn(sA, pick3(det, A));
+    R.a1 = __fdiv_rn(__fsub_rn(s1, pick3(det, D1)), sdd);
+    R.a2 = __fdiv_rn(__fsub_rn(s2, pick3(det, D2)), sdd);
+    R.b1 = fmaf(-R.a1, sA, s1);
+    R.b2 = fmaf(-R.a2, sA, s2);
+    R.corr = __fsqrt_rn(__fadd_rn(fmaf(__fmul_rn(R.a1, R.a1), sc1, __fmul_rn(__fmul_rn(R.a2, R.a2), sc2)), 1.f));
+    return R;
+}
+
+// Bilinear sample times weight_unit() on a plane whose D2 axis has unit
+// stride, in the unified form of the texture rules: with F, S the weights
+// along the fast (D2) and slow (D1) axes and y = F S / 256,
+//   256 v = 256 t00 + S (t01 - t00) + x1 (t11 - t01) + x0 (t10 - t00)
+// with t[fast][slow], and (x1, x0) = (h, F - h) for rule 0, (h, F - d) for
+// rule 1 (h, d = y rounded half up / half down). Added into acc.
+// CHECKED: border texels read zero and the coordinate is clamped;
+// otherwise the caller guarantees all four texels lie inside the volume.
+template <bool TEX8, bool CHECKED, typename T>
+__device__ __forceinline__ float fast_sample(float acc, const T* __restrict__ row0, const T* __restrict__ row1,
+                                             bool y0ok, bool y1ok, int n2, float S, float zc, int rule1) {
+    const Split b = CHECKED ? split_coord<TEX8>(zc) : split_unclamped<TEX8>(zc);
+    float t00, t10, t01, t11;
+    if (CHECKED) {
+        const bool z0ok = (unsigned)b.i < (unsigned)n2;
+        const bool z1ok = (unsigned)(b.i + 1) < (unsigned)n2;
+        t00 = (y0ok && z0ok) ? ld(row0 + b.i) : 0.f;      // fast 0, slow 0
+        t10 = (y0ok && z1ok) ? ld(row0 + b.i + 1) : 0.f;  // fast 1, slow 0
+        t01 = (y1ok && z0ok) ? ld(row1 + b.i) : 0.f;      // fast 0, slow 1
+        t11 = (y1ok && z1ok) ? ld(row1 + b.i + 1) : 0.f;
+    } else {
+        t00 = ld(row0 + b.i);
+        t10 = ld(row0 + b.i + 1);
+        t01 = ld(row1 + b.i);
+        t11 = ld(row1 + b.i + 1);
+    }
+    const float F = b.w;
+    float x1, x0;
+    if (TEX8) {
+        const float yy = F * S * (1.f / 256.f);  // exact
+        x1 = __fadd_rd(yy + 0.5f, 12582912.f) - 12582912.f;  // round half up
+        if (rule1) {
+            const float d = -(__fadd_rd(0.5f - yy, 12582912.f) - 12582912.f);  // round half down
+            x0 = F - d;
+        } else {
+            x0 = F - x1;
+        }
+    } else {
+        x1 = F * S;
+        x0 = F - x1;
+    }
+    acc = fmaf(weight_unit<TEX8>(), t00, acc);
+    acc = fmaf(S, t01 - t00, acc);
+    acc = fmaf(x1, t11 - t01, acc);
+    acc = fmaf(x0, t10 - t00, acc);
+    return acc;
+}
+
+// Slab classification of a ray from its coordinates at the first and last
+// slice of the slab (coordinates move linearly; the float32 increments
+// drift by far less than the margins). 2 = both texels of every sample
+// inside the array, 0 = every sample reads only border zeros, 1 = mixed.
+__device__ __forceinline__ int span_class(float c0, float c1, int n) {
+    const float lo = fminf(c0, c1), hi = fmaxf(c0, c1);
+    // texel i = floor(x - 1/2) on the 1/256 grid: i >= 0 iff x >= 0.498,
+    // i + 1 <= n - 1 iff x < n - 0.502; both out iff x < -0.502 or
+    // x >= n + 0.498
+    if (lo >= 0.53f && hi <= (float)n - 0.53f) return 2;
+    if (hi < -0.53f || lo > (float)n + 0.53f) return 0;
+    return 1;
+}
+
+template <typename TV, typename TP, bool TEX8, int EPI, int PATH>
+__device__ __forceinline__ void fp_trace(const FpArgs& L, const kk_fp_angle* P, int a, int A, int D1, int D2, int rule,
+                                         bool a_fast, int r0, int c, int lane) {
     float src[3], cor[3], u[3], v[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -91,6 +218,150 @@ __global__ void __launch_bounds__(FP_TILE_R* FP_TILE_C)
         u[k] = __ldg(&P->u[k]);
         v[k] = __ldg(&P->v[k]);
     }
+    const float sc1 = L.os[3 * A + 0], sc2 = L.os[3 * A + 1], oscale = L.os[3 * A + 2];
+    const int nS = L.vn[A], n1 = L.vn[D1], n2 = L.vn[D2];
+    const int64_t sS = L.vs[A], st1 = L.vs[D1], st2 = L.vs[D2];
+    const TV* vol = (const TV*)L.vol;
+    const float half1 = 0.5f * (float)n1, half2 = 0.5f * (float)n2;
+    const float unit_inv = 1.f / weight_unit<TEX8>();
+
+    // output element of ray k (row r0 + lane + 32 k)
+    auto out_ptr = [&](int k) -> TP* {
+        const int64_t off = (int64_t)(r0 + lane + 32 * k) * L.ps[1] + (int64_t)c * L.ps[2];
+        return L.table ? (TP*)L.table[a] + off : (TP*)L.out + (int64_t)a * L.ps[0] + off;
+    };
+    RaySetup R[FP_RPT];
+    float acc[FP_RPT];
+#pragma unroll
+    for (int k = 0; k < FP_RPT; ++k) {
+        const int r = r0 + lane + 32 * k;
+        const bool valid = r < L.rows;
+        R[k] = ray_setup(src, cor, u, v, A, D1, D2, valid ? r : 0, c, sc1, sc2);
+        acc[k] = (L.additive && valid) ? ld_rw(out_ptr(k)) : 0.f;
+    }
+
+    for (int off = 0; off < nS; off += L.slab) {
+        const float t1 = __fadd_rn(__fsub_rn((float)off, 0.5f * (float)nS), 0.5f);
+        const int end = min(off + L.slab, nS);
+        const float span = (float)(end - 1 - off);
+        float yc[FP_RPT], zc[FP_RPT], val[FP_RPT];
+        int cls = 2, any = 0;
+#pragma unroll
+        for (int k = 0; k < FP_RPT; ++k) {
+            yc[k] = __fadd_rn(fmaf(R[k].a1, t1, R[k].b1), half1);
+            zc[k] = __fadd_rn(fmaf(R[k].a2, t1, R[k].b2), half2);
+            val[k] = 0.f;
+            if (PATH != 0) {
+                const int cy = span_class(yc[k], fmaf(R[k].a1, span, yc[k]), n1);
+                const int cz = span_class(zc[k], fmaf(R[k].a2, span, zc[k]), n2);
+                const int ck = min(cy, cz);
+                cls = min(cls, ck);
+                any |= ck;
+            }
+        }
+        // warp-uniform choice: skip, unchecked or checked loop
+        const bool all_in = PATH != 0 && __all_sync(0xffffffffu, cls == 2);
+        const bool all_out = PATH != 0 && !__any_sync(0xffffffffu, any != 0);
+        if (all_out) continue;  // every sample is zero; the slab adds +0
+        if (PATH == 3) {
+            // the texture unit filters: layer = slice, u = the faster and
+            // v = the slower in-slice axis; each fetch equals the
+            // reference's 3D-texture sample for these rays
+            for (int sl = off; sl < end; ++sl) {
+#pragma unroll
+                for (int k = 0; k < FP_RPT; ++k) {
+                    const float uc = a_fast ? yc[k] : zc[k];
+                    const float vc = a_fast ? zc[k] : yc[k];
+                    val[k] = __fadd_rn(val[k], tex2DLayered<float>(L.vtex, uc, vc, sl));
+                    yc[k] = __fadd_rn(yc[k], R[k].a1);
+                    zc[k] = __fadd_rn(zc[k], R[k].a2);
+                }
+            }
+        } else if (PATH == 0) {
+            for (int sl = off; sl < end; ++sl) {
+                const TV* plane = vol + (int64_t)sl * sS;
+#pragma unroll
+                for (int k = 0; k < FP_RPT; ++k) {
+                    val[k] = fmaf(weight_unit<TEX8>(),
+                                  bilinear<TEX8>(plane, st1, st2, n1, n2, yc[k], zc[k], rule, a_fast), val[k]);
+                    yc[k] = __fadd_rn(yc[k], R[k].a1);
+                    zc[k] = __fadd_rn(zc[k], R[k].a2);
+                }
+            }
+        } else if (all_in) {
+            for (int sl = off; sl < end; ++sl) {
+                const TV* plane = vol + (int64_t)sl * sS;
+                if (PATH == 2) {
+                    const Split ay = split_unclamped<TEX8>(yc[0]);
+                    const TV* row0 = plane + (int64_t)ay.i * st1;
+#pragma unroll
+                    for (int k = 0; k < FP_RPT; ++k) {
+                        val[k] = fast_sample<TEX8, false>(val[k], row0, row0 + st1, true, true, n2, ay.w, zc[k], rule);
+                        zc[k] = __fadd_rn(zc[k], R[k].a2);
+                    }
+                    const float ynext = __fadd_rn(yc[0], R[0].a1);
+#pragma unroll
+                    for (int k = 0; k < FP_RPT; ++k) yc[k] = ynext;
+                } else {
+#pragma unroll
+                    for (int k = 0; k < FP_RPT; ++k) {
+                        const Split ay = split_unclamped<TEX8>(yc[k]);
+                        const TV* row0 = plane + (int64_t)ay.i * st1;
+                        val[k] = fast_sample<TEX8, false>(val[k], row0, row0 + st1, true, true, n2, ay.w, zc[k], rule);
+                        yc[k] = __fadd_rn(yc[k], R[k].a1);
+                        zc[k] = __fadd_rn(zc[k], R[k].a2);
+                    }
+                }
+            }
+        } else {
+            for (int sl = off; sl < end; ++sl) {
+                const TV* plane = vol + (int64_t)sl * sS;
+#pragma unroll
+                for (int k = 0; k < FP_RPT; ++k) {
+                    const Split ay = split_coord<TEX8>(yc[k]);
+                    const TV* row0 = plane + (int64_t)ay.i * st1;
+                    const bool y0ok = (unsigned)ay.i < (unsigned)n1;
+                    const bool y1ok = (unsigned)(ay.i + 1) < (unsigned)n1;
+                    val[k] = fast_sample<TEX8, true>(val[k], row0, row0 + st1, y0ok, y1ok, n2, ay.w, zc[k], rule);
+                    yc[k] = __fadd_rn(yc[k], R[k].a1);
+                    zc[k] = __fadd_rn(zc[k], R[k].a2);
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < FP_RPT; ++k) {
+            // texture samples are plain values; the others carry weight_unit
+            const float sum = PATH == 3 ? val[k] : __fmul_rn(val[k], unit_inv);
+            acc[k] = fmaf(__fmul_rn(sum, R[k].corr), oscale, acc[k]);
+        }
+    }
+
+#pragma unroll
+    for (int k = 0; k < FP_RPT; ++k) {
+        if (r0 + lane + 32 * k >= L.rows) continue;
+        float out = acc[k];
+        if (EPI == FP_RESIDUAL) {
+            const int r = r0 + lane + 32 * k;
+            const int64_t e = (int64_t)a * L.ps[0] + (int64_t)r * L.ps[1] + (int64_t)c * L.ps[2];
+            out = __fmul_rn(__fsub_rn(out, __ldg(L.res_y + e)), __ldg(L.res_w + e));
+        }
+        st(out_ptr(k), out);
+    }
+}
+
+template <typename TV, typename TP, bool TEX8, int EPI>
+__global__ void __launch_bounds__(32 * FP_COLS, KK_FP_MINBLOCKS) cone_fp_kernel(const FpArgs L) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int t = blockIdx.x;
+    const int ct = t % L.col_tiles;
+    t /= L.col_tiles;
+    const int rec = t % L.n_angles;
+    const int rt = t / L.n_angles;
+    const int c = ct * FP_COLS + warp;
+    if (c >= L.cols) return;  // whole warp; the kernel has no block barrier
+
+    const kk_fp_angle* P = L.angles + rec;
+    const int a = __ldg(&P->index);  // projection written by this record
     const int A = __ldg(&P->axis);
     const int D1 = A == 1 ? 0 : 1;
     const int D2 = A == 2 ? 0 : 2;
@@ -98,70 +369,30 @@ __global__ void __launch_bounds__(FP_TILE_R* FP_TILE_C)
     // rank of the slice axis (slowest: rule 0, middle: 1, fastest: 2)
     const int rule = 2 - L.rank[A];
     const bool a_fast = L.rank[D1] < L.rank[D2];
-
-    // pixel centre: (corner + u/2) + v/2, then + c u + r v (fused as the
-    // reference's compiler fuses them)
-    float det[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const float ds = __fadd_rn(__fadd_rn(cor[k], __fmul_rn(0.5f, u[k])), __fmul_rn(0.5f, v[k]));
-        det[k] = fmaf((float)r, v[k], fmaf((float)c, u[k], ds));
-    }
-    const float sA = pick3(src, A), s1 = pick3(src, D1), s2 = pick3(src, D2);
-    const float sdd = __fsub_rn(sA, pick3(det, A));
-    const float a1 = __fdiv_rn(__fsub_rn(s1, pick3(det, D1)), sdd);
-    const float a2 = __fdiv_rn(__fsub_rn(s2, pick3(det, D2)), sdd);
-    const float b1 = fmaf(-a1, sA, s1);
-    const float b2 = fmaf(-a2, sA, s2);
-
-    const float sc1 = L.os[3 * A + 0], sc2 = L.os[3 * A + 1], oscale = L.os[3 * A + 2];
-    const float corr = __fsqrt_rn(
-        __fadd_rn(fmaf(__fmul_rn(a1, a1), sc1, __fmul_rn(__fmul_rn(a2, a2), sc2)), 1.f));
-
-    const int nS = L.vn[A], n1 = L.vn[D1], n2 = L.vn[D2];
-    const int64_t sS = L.vs[A], st1 = L.vs[D1], st2 = L.vs[D2];
-    const TV* vol = (const TV*)L.vol;
-    const float half1 = 0.5f * (float)n1, half2 = 0.5f * (float)n2;
-
-    // output element
-    TP* outp;
-    {
-        const int64_t off = (int64_t)r * L.ps[1] + (int64_t)c * L.ps[2];
-        if (L.table)
-            outp = (TP*)L.table[a] + off;
-        else
-            outp = (TP*)L.out + (int64_t)a * L.ps[0] + off;
-    }
-    float acc = L.additive ? ld_rw(outp) : 0.f;
-
-    for (int off = 0; off < nS; off += L.slab) {
-        const float t1 = __fadd_rn(__fsub_rn((float)off, 0.5f * (float)nS), 0.5f);
-        float y = __fadd_rn(fmaf(a1, t1, b1), half1);
-        float z = __fadd_rn(fmaf(a2, t1, b2), half2);
-        const int end = min(off + L.slab, nS);
-        float val = 0.f;
-        for (int sl = off; sl < end; ++sl) {
-            val = __fadd_rn(val, bilinear<TEX8>(vol + (int64_t)sl * sS, st1, st2, n1, n2, y, z, rule, a_fast));
-            y = __fadd_rn(y, a1);
-            z = __fadd_rn(z, a2);
-        }
-        val = __fmul_rn(val, corr);
-        acc = fmaf(val, oscale, acc);
-    }
-
-    if (EPI == FP_RESIDUAL) {
-        const int64_t e = (int64_t)a * L.ps[0] + (int64_t)r * L.ps[1] + (int64_t)c * L.ps[2];
-        acc = __fmul_rn(__fsub_rn(acc, __ldg(L.res_y + e)), __ldg(L.res_w + e));
-    }
-    st(outp, acc);
+    const bool fast = L.vs[D2] == 1 && rule < 2;
+    const bool shared = fast && __ldg(&P->v[A]) == 0.f && __ldg(&P->v[D1]) == 0.f;
+    const int r0 = rt * FP_ROWS_T;
+    if (L.vtex && L.rank[A] == 2)
+        fp_trace<TV, TP, TEX8, EPI, 3>(L, P, a, A, D1, D2, rule, a_fast, r0, c, lane);
+    else if (shared)
+        fp_trace<TV, TP, TEX8, EPI, 2>(L, P, a, A, D1, D2, rule, a_fast, r0, c, lane);
+    else if (fast)
+        fp_trace<TV, TP, TEX8, EPI, 1>(L, P, a, A, D1, D2, rule, a_fast, r0, c, lane);
+    else
+        fp_trace<TV, TP, TEX8, EPI, 0>(L, P, a, A, D1, D2, rule, a_fast, r0, c, lane);
 }
 
 // ---------------------------------------------------------------------------
 // backprojection: one thread per (fast, middle) voxel column and a group of
 // BP_GROUP voxels along the slowest memory axis
 // ---------------------------------------------------------------------------
-template <typename TP, typename TV, bool TEX8, int EPI>
+template <typename TP, typename TV, bool TEX8, int EPI, int FETCH>
 __global__ void __launch_bounds__(BP_TILE_2* BP_TILE_1) cone_bp_kernel(const BpArgs L) {
+    // One launch covers the angles [j_begin, j_end): one 32-angle chunk,
+    // as one launch of the reference does (kernels/cone_bp.py:297-302), so
+    // the chunk's projections stay in L2 while every voxel reads them; the
+    // running sum vol += acc * scale is carried between launches in the
+    // volume (float32) or in the float32 work buffer.
     __shared__ kk_bp_angle sp[BP_CHUNK];
     const int i2 = blockIdx.x * BP_TILE_2 + threadIdx.x;
     const int i1 = blockIdx.y * BP_TILE_1 + threadIdx.y;
@@ -181,17 +412,26 @@ __global__ void __launch_bounds__(BP_TILE_2* BP_TILE_1) cone_bp_kernel(const BpA
     TV* vol = (TV*)L.vol;
     const int64_t vbase = (int64_t)g0 * L.vs[L.m0] + (int64_t)i1 * L.vs[L.m1] + (int64_t)i2 * L.vs[L.m2];
     const int64_t vstep = L.vs[L.m0];
+    // the work buffer is dense in the volume's memory order
+    const int64_t wbase = ((int64_t)g0 * n1 + i1) * n2 + i2;
+    const int64_t wstep = (int64_t)n1 * n2;
 
     float acc[BP_GROUP], vacc[BP_GROUP];
 #pragma unroll
     for (int i = 0; i < BP_GROUP; ++i) {
         acc[i] = 0.f;
-        vacc[i] = (EPI == BP_STORE && L.additive && active && i < cnt) ? ld_rw(vol + vbase + i * vstep) : 0.f;
+        vacc[i] = 0.f;
+        if (active && i < cnt) {
+            if (L.load_mode == LOAD_VOL)
+                vacc[i] = ld_rw(vol + vbase + i * vstep);
+            else if (L.load_mode == LOAD_WORK)
+                vacc[i] = L.work[wbase + i * wstep];
+        }
     }
 
     const int tid = threadIdx.y * BP_TILE_2 + threadIdx.x;
-    for (int j0 = 0; j0 < L.n_angles; j0 += BP_CHUNK) {
-        const int nj = min(BP_CHUNK, L.n_angles - j0);
+    for (int j0 = L.j_begin; j0 < L.j_end; j0 += BP_CHUNK) {
+        const int nj = min(BP_CHUNK, L.j_end - j0);
         __syncthreads();
         for (int k = tid; k < nj * 12; k += BP_TILE_2 * BP_TILE_1)
             ((float*)sp)[k] = __ldg((const float*)(L.angles + j0) + k);
@@ -200,7 +440,8 @@ __global__ void __launch_bounds__(BP_TILE_2* BP_TILE_1) cone_bp_kernel(const BpA
         for (int jj = 0; jj < nj; ++jj) {
             const kk_bp_angle& q = sp[jj];
             const int j = j0 + jj;
-            const TP* plane = L.table ? (const TP*)L.table[j] : (const TP*)L.proj + (int64_t)j * L.ps[0];
+            const TP* plane = FETCH == FETCH_TEX ? nullptr
+                              : (L.table ? (const TP*)L.table[j] : (const TP*)L.proj + (int64_t)j * L.ps[0]);
             float nu = fmaf(Z, q.num_u[2], fmaf(Y, q.num_u[1], fmaf(X, q.num_u[0], q.num_u[3])));
             float nv = fmaf(Z, q.num_v[2], fmaf(Y, q.num_v[1], fmaf(X, q.num_v[0], q.num_v[3])));
             float dn = fmaf(Z, q.den[2], fmaf(Y, q.den[1], fmaf(X, q.den[0], q.den[3])));
@@ -211,7 +452,11 @@ __global__ void __launch_bounds__(BP_TILE_2* BP_TILE_1) cone_bp_kernel(const BpA
                     const float rr = __fdividef(1.f, dn);
                     const float U = __fmul_rn(nu, rr);
                     const float V = __fmul_rn(nv, rr);
-                    const float val = bilinear<TEX8>(plane, L.ps[1], L.ps[2], L.rows, L.cols, V, U);
+                    float val;
+                    if (FETCH == FETCH_TEX)  // the hardware filter the reference samples with
+                        val = tex2DLayered<float>(L.tex, U, V, j);
+                    else
+                        val = bilinear<TEX8>(plane, L.ps[1], L.ps[2], L.rows, L.cols, V, U);
                     acc[i] = fmaf(__fmul_rn(rr, rr), val, acc[i]);
                 }
                 nu = __fadd_rn(nu, du);
@@ -230,7 +475,9 @@ __global__ void __launch_bounds__(BP_TILE_2* BP_TILE_1) cone_bp_kernel(const BpA
     for (int i = 0; i < BP_GROUP; ++i) {
         if (i >= cnt) break;
         TV* p = vol + vbase + i * vstep;
-        if (EPI == BP_UPDATE) {
+        if (L.store_mode == STORE_WORK) {
+            L.work[wbase + i * wstep] = vacc[i];
+        } else if (EPI == BP_UPDATE) {
             const int64_t e = vbase + i * vstep;
             float x = ld_rw(p);
             x = __fsub_rn(x, __fmul_rn(vacc[i], __ldg(L.upd_scale + e)));
@@ -283,25 +530,22 @@ static int check_projections(const kk_projections* p, const char* who) {
 }
 
 template <typename TV, typename TP, int EPI>
-static void launch_fp_typed(const FpArgs& base, int n_angles, bool tex8, cudaStream_t s) {
-    const int tiles = ((base.rows + FP_TILE_R - 1) / FP_TILE_R) * ((base.cols + FP_TILE_C - 1) / FP_TILE_C);
-    for (int a0 = 0; a0 < n_angles; a0 += MAX_GRID_Y) {
-        FpArgs L = base;
-        L.angle0 = a0;
-        dim3 grid(tiles, min(MAX_GRID_Y, n_angles - a0));
-        dim3 block(FP_TILE_R, FP_TILE_C);
-        if (tex8)
-            cone_fp_kernel<TV, TP, true, EPI><<<grid, block, 0, s>>>(L);
-        else
-            cone_fp_kernel<TV, TP, false, EPI><<<grid, block, 0, s>>>(L);
-    }
+static void launch_fp_typed(const FpArgs& base, bool tex8, cudaStream_t s) {
+    FpArgs L = base;
+    L.col_tiles = (L.cols + FP_COLS - 1) / FP_COLS;
+    const int row_tiles = (L.rows + FP_ROWS_T - 1) / FP_ROWS_T;
+    const int64_t blocks = (int64_t)row_tiles * L.n_angles * L.col_tiles;  // < 2^31: checked by the caller
+    if (tex8)
+        cone_fp_kernel<TV, TP, true, EPI><<<(unsigned)blocks, 32 * FP_COLS, 0, s>>>(L);
+    else
+        cone_fp_kernel<TV, TP, false, EPI><<<(unsigned)blocks, 32 * FP_COLS, 0, s>>>(L);
 }
 
 template <int EPI>
 static int launch_fp(const FpArgs& L, int n_angles, int vdt, int pdt, bool tex8, cudaStream_t s) {
 #define KK_FP_CASE(VD, PD, TV, TP)                                   \
     if (vdt == VD && pdt == PD) {                                    \
-        launch_fp_typed<TV, TP, EPI>(L, n_angles, tex8, s);          \
+        launch_fp_typed<TV, TP, EPI>(L, tex8, s);                    \
         return kk_check_launch("kk_cone_fp");                         \
     }
     KK_FP_CASE(KK_F32, KK_F32, float, float)
@@ -339,9 +583,13 @@ static int fill_fp_args(FpArgs& L, const kk_volume* vol, const kk_projections* p
     L.table = proj->table;
     L.rows = (int)proj->rows;
     L.cols = (int)proj->cols;
+    L.n_angles = (int)proj->n_angles;
     L.angles = angles;
     for (int k = 0; k < 9; ++k) L.os[k] = out_scale[k];
     L.slab = slab > 0 ? slab : FP_SLAB;
+    if ((int64_t)((L.rows + FP_ROWS_T - 1) / FP_ROWS_T) * L.n_angles * ((L.cols + FP_COLS - 1) / FP_COLS) >=
+        0x7fffffffLL)
+        return kk_fail(KK_ERR_UNSUPPORTED, "%s: too many projection tiles for one launch", who);
     for (int k = 0; k < 3; ++k) {
         L.rank[k] = 0;
         for (int j = 0; j < 3; ++j)
@@ -379,25 +627,87 @@ extern "C" int kk_cone_fp_residual(const kk_volume* vol, const kk_projections* o
                                   (cudaStream_t)stream);
 }
 
+extern "C" int kk_cone_fp_layered(const kk_layered* vtex, const kk_volume* vol, const kk_projections* proj,
+                                  const kk_fp_angle* angles, const float* out_scale,
+                                  const kk_fp_residual* residual, int32_t slab, int32_t additive, void* stream) {
+    const char* who = "kk_cone_fp_layered";
+    FpArgs L;
+    int rc = fill_fp_args(L, vol, proj, angles, out_scale, KK_INTERP_TEX8, slab, who);
+    if (rc) return rc;
+    if (!vtex) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: texture is NULL", who);
+    // the texture holds the volume with one layer per slice of the slowest
+    // axis, rows along the middle axis and columns along the fastest
+    int ax_of_rank[3];
+    for (int k = 0; k < 3; ++k) ax_of_rank[L.rank[k]] = k;
+    if (vtex->layers != vol->shape[ax_of_rank[2]] || vtex->height != vol->shape[ax_of_rank[1]] ||
+        vtex->width != vol->shape[ax_of_rank[0]])
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: texture extent differs from the volume", who);
+    if ((vol->dtype == KK_F32) != (vtex->dtype == KK_F32))
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: texture and volume storage differ", who);
+    L.vtex = vtex->tex;
+    L.additive = additive ? 1 : 0;
+    if (residual) {
+        if (!residual->y || !residual->weight)
+            return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: residual operands are NULL", who);
+        if (proj->table || proj->dtype != KK_F32 || vol->dtype != KK_F32)
+            return kk_fail(KK_ERR_UNSUPPORTED, "%s: residual epilogue needs float32 strided data", who);
+        L.res_y = residual->y;
+        L.res_w = residual->weight;
+        return launch_fp<FP_RESIDUAL>(L, (int)proj->n_angles, vol->dtype, proj->dtype, true, (cudaStream_t)stream);
+    }
+    return launch_fp<FP_STORE>(L, (int)proj->n_angles, vol->dtype, proj->dtype, true, (cudaStream_t)stream);
+}
+
 // ---------------------------------------------------------------------------
+
+static dim3 bp_grid(const BpArgs& L) {
+    return dim3((L.vn[L.m2] + BP_TILE_2 - 1) / BP_TILE_2, (L.vn[L.m1] + BP_TILE_1 - 1) / BP_TILE_1,
+                (L.vn[L.m0] + BP_GROUP - 1) / BP_GROUP);
+}
 
 template <typename TP, typename TV, int EPI>
 static void launch_bp_typed(const BpArgs& L, bool tex8, cudaStream_t s) {
     dim3 block(BP_TILE_2, BP_TILE_1);
-    dim3 grid((L.vn[L.m2] + BP_TILE_2 - 1) / BP_TILE_2, (L.vn[L.m1] + BP_TILE_1 - 1) / BP_TILE_1,
-              (L.vn[L.m0] + BP_GROUP - 1) / BP_GROUP);
     if (tex8)
-        cone_bp_kernel<TP, TV, true, EPI><<<grid, block, 0, s>>>(L);
+        cone_bp_kernel<TP, TV, true, EPI, FETCH_GLOBAL><<<bp_grid(L), block, 0, s>>>(L);
     else
-        cone_bp_kernel<TP, TV, false, EPI><<<grid, block, 0, s>>>(L);
+        cone_bp_kernel<TP, TV, false, EPI, FETCH_GLOBAL><<<bp_grid(L), block, 0, s>>>(L);
+}
+
+// Launch `one` once per 32-angle chunk. The running sum lives in the volume
+// when it is float32 and the result is a plain sum; otherwise in the
+// float32 work buffer (when given). Without a buffer in those cases a
+// single launch covers every angle (same arithmetic, more L2 traffic).
+template <typename Fn>
+static void bp_chunks(BpArgs L, bool vol_f32, bool additive, bool update, Fn one) {
+    const int n = L.n_angles;
+    const int chunks = (n + BP_CHUNK - 1) / BP_CHUNK;
+    const bool need_work = chunks > 1 && (!vol_f32 || update);
+    const int first_load = (additive && !update) ? LOAD_VOL : LOAD_ZERO;
+    if (need_work && !L.work) {
+        L.j_begin = 0;
+        L.j_end = n;
+        L.load_mode = first_load;
+        L.store_mode = STORE_FINAL;
+        one(L);
+        return;
+    }
+    for (int c = 0; c < chunks; ++c) {
+        L.j_begin = c * BP_CHUNK;
+        L.j_end = min(n, L.j_begin + BP_CHUNK);
+        L.load_mode = c == 0 ? first_load : (need_work ? LOAD_WORK : LOAD_VOL);
+        L.store_mode = c == chunks - 1 ? STORE_FINAL : (need_work ? STORE_WORK : STORE_VOL);
+        one(L);
+    }
 }
 
 template <int EPI>
-static int launch_bp(const BpArgs& L, int pdt, int vdt, bool tex8, cudaStream_t s) {
-#define KK_BP_CASE(PD, VD, TP, TV)                          \
-    if (pdt == PD && vdt == VD) {                           \
-        launch_bp_typed<TP, TV, EPI>(L, tex8, s);           \
-        return kk_check_launch("kk_cone_bp");                \
+static int launch_bp(const BpArgs& L, int pdt, int vdt, bool tex8, bool additive, cudaStream_t s) {
+#define KK_BP_CASE(PD, VD, TP, TV)                                                                  \
+    if (pdt == PD && vdt == VD) {                                                                   \
+        bp_chunks(L, VD == KK_F32, additive, EPI == BP_UPDATE,                                      \
+                  [&](const BpArgs& c) { launch_bp_typed<TP, TV, EPI>(c, tex8, s); });             \
+        return kk_check_launch("kk_cone_bp");                                                      \
     }
     KK_BP_CASE(KK_F32, KK_F32, float, float)
     if (EPI == BP_STORE) {
@@ -456,16 +766,18 @@ static int fill_bp_args(BpArgs& L, const kk_projections* proj, const kk_volume* 
 }
 
 extern "C" int kk_cone_bp(const kk_projections* proj, const kk_volume* vol, const kk_bp_angle* angles,
-                          float out_scale, int32_t interp, int32_t additive, void* stream) {
+                          float out_scale, int32_t interp, int32_t additive, float* work, void* stream) {
     BpArgs L;
     int rc = fill_bp_args(L, proj, vol, angles, out_scale, interp, "kk_cone_bp");
     if (rc) return rc;
-    L.additive = additive ? 1 : 0;
-    return launch_bp<BP_STORE>(L, proj->dtype, vol->dtype, interp == KK_INTERP_TEX8, (cudaStream_t)stream);
+    L.work = work;
+    return launch_bp<BP_STORE>(L, proj->dtype, vol->dtype, interp == KK_INTERP_TEX8, additive != 0,
+                               (cudaStream_t)stream);
 }
 
 extern "C" int kk_cone_bp_update(const kk_projections* proj, const kk_volume* vol, const kk_bp_angle* angles,
-                                 float out_scale, const kk_bp_update* update, int32_t interp, void* stream) {
+                                 float out_scale, const kk_bp_update* update, int32_t interp, float* work,
+                                 void* stream) {
     BpArgs L;
     int rc = fill_bp_args(L, proj, vol, angles, out_scale, interp, "kk_cone_bp_update");
     if (rc) return rc;
@@ -479,5 +791,137 @@ extern "C" int kk_cone_bp_update(const kk_projections* proj, const kk_volume* vo
     L.vmax = update->max_value;
     L.has_min = update->has_min;
     L.has_max = update->has_max;
-    return launch_bp<BP_UPDATE>(L, proj->dtype, vol->dtype, interp == KK_INTERP_TEX8, (cudaStream_t)stream);
+    L.work = work;
+    return launch_bp<BP_UPDATE>(L, proj->dtype, vol->dtype, interp == KK_INTERP_TEX8, false, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+// layered texture of the projections (reference: the 2D-layered CUDA array
+// BackProjector samples with, projector.py:529-542 and kernel.py:91-96)
+// ---------------------------------------------------------------------------
+
+extern "C" int kk_layered_create(int64_t layers, int64_t height, int64_t width, int32_t dtype, kk_layered** out) {
+    if (!out) return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_layered_create: out is NULL");
+    *out = nullptr;
+    if (layers <= 0 || height <= 0 || width <= 0 || layers > 2048 || height >= (int64_t)COORD_LIMIT ||
+        width >= (int64_t)COORD_LIMIT)
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_layered_create: bad extent (%lld, %lld, %lld)",
+                       (long long)layers, (long long)height, (long long)width);
+    if (dtype != KK_F32 && dtype != KK_F16)
+        return kk_fail(KK_ERR_UNSUPPORTED, "kk_layered_create: float32 or float16 texels only");
+    cudaChannelFormatDesc ch = dtype == KK_F32 ? cudaCreateChannelDesc<float>() : cudaCreateChannelDescHalf();
+    kk_layered* t = new kk_layered();
+    t->layers = layers;
+    t->height = height;
+    t->width = width;
+    t->dtype = dtype;
+    cudaError_t e = cudaMalloc3DArray(&t->array, &ch, make_cudaExtent(width, height, layers), cudaArrayLayered);
+    if (e != cudaSuccess) {
+        delete t;
+        return kk_fail(KK_ERR_CUDA, "kk_layered_create: %s", cudaGetErrorString(e));
+    }
+    cudaResourceDesc rd = {};
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = t->array;
+    cudaTextureDesc td = {};
+    td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeBorder;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    e = cudaCreateTextureObject(&t->tex, &rd, &td, nullptr);
+    if (e != cudaSuccess) {
+        cudaFreeArray(t->array);
+        delete t;
+        return kk_fail(KK_ERR_CUDA, "kk_layered_create: %s", cudaGetErrorString(e));
+    }
+    *out = t;
+    return KK_OK;
+}
+
+extern "C" int kk_layered_destroy(kk_layered* t) {
+    if (!t) return KK_OK;
+    cudaDestroyTextureObject(t->tex);
+    cudaFreeArray(t->array);
+    delete t;
+    return KK_OK;
+}
+
+extern "C" int kk_layered_copy(kk_layered* t, const kk_projections* src, void* stream) {
+    if (!t || !src) return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_layered_copy: NULL argument");
+    if (src->table || !src->data)
+        return kk_fail(KK_ERR_UNSUPPORTED, "kk_layered_copy: strided projections only");
+    if (src->n_angles != t->layers || src->rows != t->height || src->cols != t->width || src->dtype != t->dtype)
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_layered_copy: shape or dtype differs from the texture");
+    const size_t es = t->dtype == KK_F32 ? 4 : 2;
+    if (src->stride[2] != 1 || src->stride[0] != src->rows * src->stride[1])
+        return kk_fail(KK_ERR_UNSUPPORTED, "kk_layered_copy: rows must be contiguous and angles dense");
+    cudaMemcpy3DParms cp = {};
+    cp.srcPtr = make_cudaPitchedPtr(src->data, (size_t)src->stride[1] * es, (size_t)src->cols, (size_t)src->rows);
+    cp.dstArray = t->array;
+    cp.extent = make_cudaExtent(t->width, t->height, t->layers);
+    cp.kind = cudaMemcpyDeviceToDevice;
+    cudaError_t e = cudaMemcpy3DAsync(&cp, (cudaStream_t)stream);
+    if (e != cudaSuccess) return kk_fail(KK_ERR_CUDA, "kk_layered_copy: %s", cudaGetErrorString(e));
+    return KK_OK;
+}
+
+static int layered_args(BpArgs& L, const kk_layered* t, const kk_volume* vol, const kk_bp_angle* angles,
+                        float out_scale, const char* who) {
+    if (!t) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: texture is NULL", who);
+    kk_projections p = {};
+    p.data = (void*)1;  // texels come from the texture; the descriptor carries the extent
+    p.n_angles = t->layers;
+    p.rows = t->height;
+    p.cols = t->width;
+    p.stride[0] = t->height * t->width;
+    p.stride[1] = t->width;
+    p.stride[2] = 1;
+    p.dtype = KK_F32;
+    int rc = fill_bp_args(L, &p, vol, angles, out_scale, KK_INTERP_TEX8, who);
+    if (rc) return rc;
+    L.proj = nullptr;
+    L.tex = t->tex;
+    return KK_OK;
+}
+
+extern "C" int kk_cone_bp_layered(const kk_layered* t, const kk_volume* vol, const kk_bp_angle* angles,
+                                  float out_scale, int32_t additive, float* work, void* stream) {
+    BpArgs L;
+    int rc = layered_args(L, t, vol, angles, out_scale, "kk_cone_bp_layered");
+    if (rc) return rc;
+    L.work = work;
+    const dim3 block(BP_TILE_2, BP_TILE_1);
+    const cudaStream_t s = (cudaStream_t)stream;
+    const int vdt = vol->dtype;
+    bp_chunks(L, vdt == KK_F32, additive != 0, false, [&](const BpArgs& c) {
+        if (vdt == KK_F32)
+            cone_bp_kernel<float, float, true, BP_STORE, FETCH_TEX><<<bp_grid(c), block, 0, s>>>(c);
+        else if (vdt == KK_BF16)
+            cone_bp_kernel<float, __nv_bfloat16, true, BP_STORE, FETCH_TEX><<<bp_grid(c), block, 0, s>>>(c);
+        else
+            cone_bp_kernel<float, __half, true, BP_STORE, FETCH_TEX><<<bp_grid(c), block, 0, s>>>(c);
+    });
+    return kk_check_launch("kk_cone_bp_layered");
+}
+
+extern "C" int kk_cone_bp_layered_update(const kk_layered* t, const kk_volume* vol, const kk_bp_angle* angles,
+                                         float out_scale, const kk_bp_update* update, float* work, void* stream) {
+    const char* who = "kk_cone_bp_layered_update";
+    if (!update || !update->scale) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: update scale is NULL", who);
+    if (!vol || vol->dtype != KK_F32) return kk_fail(KK_ERR_UNSUPPORTED, "%s: float32 volume only", who);
+    BpArgs L;
+    int rc = layered_args(L, t, vol, angles, out_scale, who);
+    if (rc) return rc;
+    L.upd_scale = update->scale;
+    L.upd_mask = update->mask;
+    L.vmin = update->min_value;
+    L.vmax = update->max_value;
+    L.has_min = update->has_min;
+    L.has_max = update->has_max;
+    L.work = work;
+    const cudaStream_t s = (cudaStream_t)stream;
+    bp_chunks(L, true, false, true, [&](const BpArgs& c) {
+        cone_bp_kernel<float, float, true, BP_UPDATE, FETCH_TEX><<<bp_grid(c), dim3(BP_TILE_2, BP_TILE_1), 0, s>>>(c);
+    });
+    return kk_check_launch(who);
 }

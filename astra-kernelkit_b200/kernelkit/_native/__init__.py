@@ -12,8 +12,9 @@ from typing import Sequence
 
 import numpy as np
 
-LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)),
-                        "libkk.so")
+LIB_PATH = os.environ.get(
+    "KERNELKIT_LIBKK",
+    os.path.join(os.path.dirname(os.path.abspath(__file__)), "libkk.so"))
 
 KK_OK = 0
 KK_ERR_INVALID_ARGUMENT = 1
@@ -52,14 +53,18 @@ class kk_bp_update(ctypes.Structure):
 #: kk_fp_angle as a NumPy record (64 bytes)
 FP_ANGLE_DTYPE = np.dtype([("src", "<f4", 3), ("corner", "<f4", 3),
                            ("u", "<f4", 3), ("v", "<f4", 3),
-                           ("axis", "<i4"), ("pad", "<i4", 3)])
+                           ("axis", "<i4"), ("index", "<i4"),
+                           ("pad", "<i4", 2)])
 #: kk_bp_angle as a NumPy record (48 bytes)
 BP_ANGLE_DTYPE = np.dtype([("num_u", "<f4", 4), ("num_v", "<f4", 4),
                            ("den", "<f4", 4)])
 
 #: every symbol include/kk.h declares
-EXPORTS = ("kk_cone_fp", "kk_cone_fp_residual", "kk_cone_bp",
-           "kk_cone_bp_update", "kk_preweight", "kk_filter_rows",
+EXPORTS = ("kk_cone_fp", "kk_cone_fp_residual", "kk_cone_fp_layered",
+           "kk_cone_bp",
+           "kk_cone_bp_update", "kk_layered_create", "kk_layered_copy",
+           "kk_layered_destroy", "kk_cone_bp_layered",
+           "kk_cone_bp_layered_update", "kk_preweight", "kk_filter_rows",
            "kk_reciprocal", "kk_last_error", "kk_abi_version")
 
 _lib = None
@@ -86,10 +91,18 @@ def load():
                              i32, i32, vp]
     L.kk_cone_fp_residual.argtypes = [P(kk_volume), P(kk_projections), vp, vp,
                                       P(kk_fp_residual), i32, i32, vp]
+    L.kk_cone_fp_layered.argtypes = [vp, P(kk_volume), P(kk_projections), vp,
+                                     vp, P(kk_fp_residual), i32, i32, vp]
     L.kk_cone_bp.argtypes = [P(kk_projections), P(kk_volume), vp, f32, i32,
-                             i32, vp]
+                             i32, vp, vp]
     L.kk_cone_bp_update.argtypes = [P(kk_projections), P(kk_volume), vp, f32,
-                                    P(kk_bp_update), i32, vp]
+                                    P(kk_bp_update), i32, vp, vp]
+    L.kk_layered_create.argtypes = [i64, i64, i64, i32, P(vp)]
+    L.kk_layered_copy.argtypes = [vp, P(kk_projections), vp]
+    L.kk_layered_destroy.argtypes = [vp]
+    L.kk_cone_bp_layered.argtypes = [vp, P(kk_volume), vp, f32, i32, vp, vp]
+    L.kk_cone_bp_layered_update.argtypes = [vp, P(kk_volume), vp, f32,
+                                            P(kk_bp_update), vp, vp]
     L.kk_preweight.argtypes = [P(kk_projections), vp, vp]
     L.kk_filter_rows.argtypes = [P(kk_projections), vp, i64, vp]
     L.kk_reciprocal.argtypes = [vp, i64, vp]
@@ -195,3 +208,31 @@ def table_desc(table, n_angles, rows, cols, row_stride, col_stride,
 
 def ptr(t) -> int:
     return 0 if t is None else t.data_ptr()
+
+
+class Layered:
+    """Owner of a ``kk_layered`` texture (destroyed with the object)."""
+
+    def __init__(self, layers, height, width, dtype):
+        self.shape = (int(layers), int(height), int(width))
+        self.dtype = int(dtype)
+        h = ctypes.c_void_p()
+        check(load().kk_layered_create(self.shape[0], self.shape[1],
+                                       self.shape[2], self.dtype,
+                                       ctypes.byref(h)))
+        self.handle = h
+
+    def copy_from(self, t):
+        """Copy a (layers, height, width) CUDA tensor on the current
+        stream."""
+        d = projections_desc(t)
+        if (d.n_angles, d.rows, d.cols) != self.shape:
+            raise ValueError(f"Shape {tuple(t.shape)} does not match the "
+                             f"texture {self.shape}.")
+        check(load().kk_layered_copy(self.handle, d, current_stream()))
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.kk_layered_destroy(h)
+            self.handle = None

@@ -166,12 +166,23 @@ class SIRT:
                                       stream))
         del ones
         self.y_tmp = t.empty_like(self.y)
+        # the backprojection samples the residual through a layered
+        # texture (the reference's filter), refilled every iteration
+        self.tex = (_native.Layered(*self.y.shape, _native.KK_F32)
+                    if interpolation == "texture" and len(self.y) <= 2048
+                    else None)
+        self.bp._work_for(self.x, True)  # allocate before any graph capture
         self._graph = None
 
     def step(self):
-        """One iteration: two kernel launches."""
+        """One iteration: forward projection with the residual epilogue,
+        (texture refill) and backprojection with the update epilogue."""
         self.fp.residual(self.x, self.pg, self.vg, self.y_tmp, self.y, self.R)
-        self.bp.update(self.y_tmp, self.x, self.vg, self.C, self.mask,
+        src = self.y_tmp
+        if self.tex is not None:
+            self.tex.copy_from(self.y_tmp)
+            src = self.tex
+        self.bp.update(src, self.x, self.vg, self.C, self.mask,
                        self.min_c, self.max_c)
 
     def capture(self):

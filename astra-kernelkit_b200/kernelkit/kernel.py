@@ -39,10 +39,20 @@ class Texture:
     array: object
     texture_type: str = "array"
     layered: bool = False
+    _layered: object = None
 
     @property
     def shape(self):
         return tuple(self.array.shape)
+
+    def layered_texture(self):
+        """The 2D-layered texture (one layer per entry of the first axis)
+        of a 3D float32/float16 array, made on first use."""
+        if self._layered is None:
+            self._layered = _native.Layered(*self.array.shape,
+                                            _native.dtype_code(self.array))
+            self._layered.copy_from(self.array)
+        return self._layered
 
 
 def copy_to_texture(array, texture_type: str = "array",

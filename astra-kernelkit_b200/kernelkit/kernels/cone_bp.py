@@ -126,6 +126,33 @@ class VoxelDrivenConeBP(BaseKernel):
         self._params_dev = t.from_numpy(arr.reshape(-1)).cuda()
         self._n_params = arr.size // 12
 
+    def _work_for(self, vol, update: bool):
+        """float32 running-sum buffer for chunked launches (one element per
+        voxel), made on first use; 0 when the volume itself can hold the
+        running sum."""
+        t = _arrays.torch()
+        if self._n_params <= 32 or (vol.dtype == t.float32 and not update):
+            return 0
+        w = getattr(self, "_work", None)
+        if w is None or w.numel() != vol.numel() or w.device != vol.device:
+            w = t.empty(vol.numel(), dtype=t.float32, device=vol.device)
+            self._work = w
+        return w.data_ptr()
+
+    def _layered_source(self, textures):
+        """The layered texture to sample, or None for the device-memory
+        path: texture interpolation is only the reference's own filter,
+        for angle-first projections."""
+        t = _arrays.torch()
+        if self._interp != _native.KK_INTERP_TEX8 or self._proj_axs[0] != 0:
+            return None
+        if isinstance(textures, _native.Layered):
+            return textures
+        if (isinstance(textures, Texture) and textures.array.dim() == 3
+                and textures.array.dtype == t.float32):
+            return textures.layered_texture()
+        return None
+
     def _input(self, textures):
         t = _arrays.torch()
         if isinstance(textures, Texture):
@@ -146,9 +173,10 @@ class VoxelDrivenConeBP(BaseKernel):
 
         As in the reference the result is added to ``volume``; pass
         ``additive=False`` to overwrite instead. ``textures`` is a
-        ``Texture``, a device array laid out by ``projection_axes`` or a
-        list of 2D device arrays; ``volume`` a C-contiguous device array
-        laid out by ``volume_axes``."""
+        ``Texture`` (sampled through its layered texture, i.e. the
+        reference's own filter), a layered texture, a device array laid out
+        by ``projection_axes`` or a list of 2D device arrays; ``volume`` a
+        C-contiguous device array laid out by ``volume_axes``."""
         t = _arrays.torch()
         if not _arrays.is_device_array(volume):
             raise TypeError("`volume` must be a device array.")
@@ -167,18 +195,29 @@ class VoxelDrivenConeBP(BaseKernel):
         if not self.is_compiled:
             raise KernelNotCompiledException(
                 "Please compile the kernel with `compile()`.")
-        pdesc, keep = self._input(textures)
+        vdesc = _native.volume_desc(vol, self._vol_axs)
+        vox_vol = np.float32(volume_geometry.voxel_volume())
+        lay = self._layered_source(textures)
         if not self._params_are_set:
             raise KernelMemoryUnpreparedException(
                 "Please set the parameters with `set_params()`.")
+        if lay is not None:
+            if lay.shape[0] != self._n_params:
+                raise ValueError(f"{lay.shape[0]} projections given, but "
+                                 f"parameters for {self._n_params} angles.")
+            _native.check(_native.load().kk_cone_bp_layered(
+                lay.handle, vdesc, self._params_dev.data_ptr(),
+                float(vox_vol), int(bool(additive)),
+                self._work_for(vol, False), _native.current_stream()))
+            return
+        pdesc, keep = self._input(textures)
         if pdesc.n_angles != self._n_params:
             raise ValueError(f"{pdesc.n_angles} projections given, but "
                              f"parameters for {self._n_params} angles.")
-        vdesc = _native.volume_desc(vol, self._vol_axs)
-        vox_vol = np.float32(volume_geometry.voxel_volume())
         _native.check(_native.load().kk_cone_bp(
             pdesc, vdesc, self._params_dev.data_ptr(), float(vox_vol),
-            self._interp, int(bool(additive)), _native.current_stream()))
+            self._interp, int(bool(additive)), self._work_for(vol, False),
+            _native.current_stream()))
         del keep
 
     def update(self, projections, volume, volume_geometry: VolumeGeometry,
@@ -190,7 +229,6 @@ class VoxelDrivenConeBP(BaseKernel):
         if not self._params_are_set:
             raise KernelMemoryUnpreparedException(
                 "Please set the parameters with `set_params()`.")
-        pdesc, keep = self._input(projections)
         vdesc = _native.volume_desc(volume, self._vol_axs)
         for name, a in (("scale", scale), ("mask", mask)):
             if a is not None and (a.shape != volume.shape
@@ -202,9 +240,18 @@ class VoxelDrivenConeBP(BaseKernel):
             float(max_value) if max_value is not None else 0.0,
             int(min_value is not None), int(max_value is not None))
         vox_vol = np.float32(volume_geometry.voxel_volume())
+        lay = self._layered_source(projections)
+        if lay is not None:
+            _native.check(_native.load().kk_cone_bp_layered_update(
+                lay.handle, vdesc, self._params_dev.data_ptr(),
+                float(vox_vol), upd, self._work_for(volume, True),
+                _native.current_stream()))
+            return
+        pdesc, keep = self._input(projections)
         _native.check(_native.load().kk_cone_bp_update(
             pdesc, vdesc, self._params_dev.data_ptr(), float(vox_vol), upd,
-            self._interp, _native.current_stream()))
+            self._interp, self._work_for(volume, True),
+            _native.current_stream()))
         del keep
 
     @staticmethod

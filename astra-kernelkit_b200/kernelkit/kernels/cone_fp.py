@@ -113,8 +113,14 @@ class RayDrivenConeFP(BaseKernel):
                  slices_per_block: int = None,
                  volume_axes: tuple = (0, 1, 2),
                  projection_axes: tuple = (0, 1, 2),
-                 interpolation: str = "texture"):
+                 interpolation: str = "texture",
+                 use_texture_unit: bool = True):
         super().__init__()
+        # rays along the volume's slowest axis may sample a layered copy of
+        # the volume through the texture unit (same filter as the
+        # reference); the others run on the CUDA cores
+        self.use_texture_unit = bool(use_texture_unit)
+        self._vtex = None
         if pixels_per_block is not None:
             self.pixels_per_block = tuple(pixels_per_block)
         if slices_per_block is not None:
@@ -214,10 +220,23 @@ class RayDrivenConeFP(BaseKernel):
         axes = getattr(params, "axes", None)
         self._axes_known = axes is not None
         rec["axis"] = axes if axes is not None else 0
+        rec["index"] = np.arange(n)
         self._host_params = rec
-        t = _arrays.torch()
-        self._params_dev = t.from_numpy(rec.view(np.uint8)).cuda()
+        self._upload()
         self._n_params = n
+
+    def _upload(self):
+        """Upload the records interleaved by ray axis, so that every part
+        of the launch mixes texture-unit and CUDA-core work."""
+        rec = self._host_params
+        key = np.empty(len(rec))
+        for ax in range(3):
+            sel = np.flatnonzero(rec["axis"] == ax)
+            key[sel] = (np.arange(len(sel)) + 0.5) / max(len(sel), 1)
+        order = np.argsort(key, kind="stable")
+        t = _arrays.torch()
+        self._params_dev = t.from_numpy(
+            np.ascontiguousarray(rec[order]).view(np.uint8)).cuda()
 
     def _ensure_axes(self, projection_geometry, volume_geometry):
         if self._axes_known:
@@ -225,10 +244,30 @@ class RayDrivenConeFP(BaseKernel):
         pg = _sequence(projection_geometry)
         normalize_(pg, volume_geometry)
         self._host_params["axis"] = self._geom_axes(pg)
-        t = _arrays.torch()
-        self._params_dev = t.from_numpy(self._host_params.view(np.uint8)
-                                        ).cuda()
+        self._upload()
         self._axes_known = True
+
+    def _volume_texture(self, vol, vdesc):
+        """Layered texture of ``vol`` (one layer per slice of its slowest
+        axis), refilled from ``vol``; None when the texture unit is not
+        used for this call."""
+        t = _arrays.torch()
+        # float32 only: the texture unit filters 16-bit texels in reduced
+        # precision, while the reference's arithmetic is float32
+        if (not self.use_texture_unit or self._interp != _native.KK_INTERP_TEX8
+                or vol.dtype != t.float32
+                or not vol.is_contiguous() or vol.shape[0] > 2048):
+            return None
+        slowest = self._vol_axs[0]
+        if not np.any(self._host_params["axis"] == slowest):
+            return None
+        code = _native.dtype_code(vol)
+        lay = self._vtex
+        if lay is None or lay.shape != tuple(vol.shape) or lay.dtype != code:
+            lay = _native.Layered(*vol.shape, code)
+            self._vtex = lay
+        lay.copy_from(vol)
+        return lay
 
     # -- launch -------------------------------------------------------------
     def _output(self, projections, projection_geometry, projections_pitch):
@@ -308,10 +347,17 @@ class RayDrivenConeFP(BaseKernel):
         osc = np.asarray(self._output_scale(volume_geometry.voxel_size),
                          np.float32).reshape(9)
         L = _native.load()
-        _native.check(L.kk_cone_fp(
-            vdesc, pdesc, self._params_dev.data_ptr(), osc.ctypes.data,
-            self._interp, self.slices_per_block, int(bool(additive)),
-            _native.current_stream()))
+        lay = self._volume_texture(vol, vdesc)
+        if lay is not None:
+            _native.check(L.kk_cone_fp_layered(
+                lay.handle, vdesc, pdesc, self._params_dev.data_ptr(),
+                osc.ctypes.data, None, self.slices_per_block,
+                int(bool(additive)), _native.current_stream()))
+        else:
+            _native.check(L.kk_cone_fp(
+                vdesc, pdesc, self._params_dev.data_ptr(), osc.ctypes.data,
+                self._interp, self.slices_per_block, int(bool(additive)),
+                _native.current_stream()))
         del keep
 
     def residual(self, volume, projection_geometry,
@@ -331,6 +377,13 @@ class RayDrivenConeFP(BaseKernel):
         res = _native.kk_fp_residual(measured.data_ptr(), weight.data_ptr())
         osc = np.asarray(self._output_scale(volume_geometry.voxel_size),
                          np.float32).reshape(9)
+        lay = self._volume_texture(volume, vdesc)
+        if lay is not None:
+            _native.check(_native.load().kk_cone_fp_layered(
+                lay.handle, vdesc, pdesc, self._params_dev.data_ptr(),
+                osc.ctypes.data, res, self.slices_per_block, 0,
+                _native.current_stream()))
+            return
         _native.check(_native.load().kk_cone_fp_residual(
             vdesc, pdesc, self._params_dev.data_ptr(), osc.ctypes.data, res,
             self._interp, self.slices_per_block, _native.current_stream()))

@@ -80,6 +80,43 @@ def voxelize(ell: Ellipsoids, shape, extent_min, voxel_size,
     return vol.astype(dtype)
 
 
+def voxelize_torch(ell: Ellipsoids, shape, extent_min, voxel_size,
+                   device="cuda", dtype=None):
+    """``voxelize`` evaluated with PyTorch on ``device`` (float64 geometry,
+    same inclusion rule), for large volumes. Returns a float32 tensor
+    ``vol[x, y, z]``."""
+    import torch
+
+    dtype = dtype or torch.float32
+    shape = tuple(int(s) for s in shape)
+    vs = np.asarray(voxel_size, np.float64).reshape(3)
+    lo = np.asarray(extent_min, np.float64).reshape(3)
+    vol = torch.zeros(shape, dtype=torch.float32, device=device)
+    for c, a, R, d in zip(ell.centers, ell.semi_axes, ell.rotations,
+                          ell.densities):
+        ext = np.sqrt(((R * a[None, :]) ** 2).sum(axis=1))
+        sl = []
+        for i in range(3):
+            i0 = max(0, int(np.floor((c[i] - ext[i] - lo[i]) / vs[i])) - 1)
+            i1 = min(shape[i], int(np.ceil((c[i] + ext[i] - lo[i]) / vs[i]))
+                     + 1)
+            sl.append((i0, i1))
+        if any(i0 >= i1 for i0, i1 in sl):
+            continue
+        ax = [torch.arange(i0, i1, dtype=torch.float64, device=device)
+              for (i0, i1) in sl]
+        X = (lo[0] + (ax[0] + 0.5) * vs[0] - c[0])[:, None, None]
+        Y = (lo[1] + (ax[1] + 0.5) * vs[1] - c[1])[None, :, None]
+        Z = (lo[2] + (ax[2] + 0.5) * vs[2] - c[2])[None, None, :]
+        q = 0.0
+        for j in range(3):
+            qj = (R[0, j] * X + R[1, j] * Y + R[2, j] * Z) / a[j]
+            q = q + qj * qj
+        vol[sl[0][0]:sl[0][1], sl[1][0]:sl[1][1], sl[2][0]:sl[2][1]] += (
+            float(d) * (q <= 1.0)).float()
+    return vol.to(dtype)
+
+
 def line_integrals(ell: Ellipsoids, sources, pixels, device="cpu",
                    chunk=1 << 22):
     """Exact FP64 line integrals through the ellipsoids.

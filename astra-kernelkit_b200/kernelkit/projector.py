@@ -3,9 +3,11 @@
 Mirrors ``kernelkit/projector.py`` of the reference: the same classes,
 properties, setter ordering (kernel parameters are pushed as soon as both
 geometries are known), ``__call__(additive)`` semantics and exceptions.
-Differences: device memory is referenced, never copied into texture
-arrays, and non-additive calls overwrite instead of zero-filling first;
-the caller's geometry objects are never normalised in place.
+Differences: the forward projector reads the volume in place (no texture
+copy); the backprojector copies projections into a layered texture only
+for the CUDA-array texture types, as the reference does; non-additive
+calls overwrite instead of zero-filling first; the caller's geometry
+objects are never normalised in place.
 """
 from __future__ import annotations
 
@@ -327,12 +329,38 @@ class BackProjector(Projector):
                 raise ValueError("Can only use a list of projections when "
                                  "projection axis is 0.")
             self._projs = [_arrays.as_tensor(p) for p in value]
+            self._layered = None
         else:
             if (self._texture_type == "layered"
                     and self._K.projection_axes[0] != 0):
                 raise ValueError("Can only use layered texture when the "
                                  "first projection axis is 0.")
             self._projs = _arrays.as_tensor(value)
+            self._layered = self._fill_texture(self._projs)
+
+    def _fill_texture(self, projs):
+        """For the texture types backed by a CUDA array ('layered',
+        'array'), copy the projections into the projector's layered
+        texture (made once per shape), as the reference copies them into
+        its CUDA array (projector.py:529-542)."""
+        t = _arrays.torch()
+        K = self._K
+        if (self._texture_type not in ("layered", "array")
+                or K.projection_axes[0] != 0
+                or K.interpolation.lower() not in ("texture", "tex8")
+                or projs.dim() != 3
+                or projs.dtype != t.float32
+                or projs.shape[0] > 2048):
+            return None
+        from . import _native
+
+        lay = getattr(self, "_layered_tex", None)
+        code = _native.dtype_code(projs)
+        if lay is None or lay.shape != tuple(projs.shape) or lay.dtype != code:
+            lay = _native.Layered(*projs.shape, code)
+            self._layered_tex = lay
+        lay.copy_from(projs.contiguous())
+        return lay
 
     @projections.deleter
     def projections(self):
@@ -344,8 +372,8 @@ class BackProjector(Projector):
     def __call__(self, additive: bool = False):
         """Backproject into the volume (overwriting it unless
         ``additive``)."""
-        self._K(self.projections, self.volume, self.volume_geometry,
-                additive=additive)
+        src = getattr(self, "_layered", None) or self.projections
+        self._K(src, self.volume, self.volume_geometry, additive=additive)
 
 
 __all__ = ["ProjectionGeometryNotSetError", "VolumeGeometryNotSetError",

@@ -1,0 +1,494 @@
+#!/usr/bin/env python
+"""Benchmark of the cone-beam hot path: forward projection + backprojection
+GUPS (giga voxel-angle updates per second) at 512^3 voxels / 720 angles /
+768^2 detector, the headline workload.
+
+One step = one forward projection of the volume over all angles plus one
+backprojection of a full sinogram, with the data resident in HBM (inputs
+larger than L2, so no flush is needed). GUPS(FP+BP) = 2 N / (t_FP + t_BP)
+with N = voxels x angles. Also reported: the same metric end to end
+through ``XrayTransform`` with the volume coming from and going back to
+pinned host memory (x -> A^T A x), a roofline entry for the dominant
+kernel, and a CPU baseline (the FP64 NumPy oracle on a bounded sample on
+the host cores). ``--impl reference`` times the reference arm, the
+oracle's restatement of the reference algorithm on all host cores.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W]
+       [--impl ours|reference] [--workload headline|config2|profile]
+Multi-GPU runs (torchrun) are independent replicas, one per GPU.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "astra-kernelkit_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "cone FP+BP GUPS @512^3/720 ang"
+UNIT = "GUPS"
+
+WORKLOADS = {
+    # 512^3, 720 angles over 2 pi, 768^2 detector, SOD 1600, SDD 3200,
+    # pitch 1.3, voxel 1.0, 200 ellipsoids (config-2 ranges scaled x2)
+    "headline": dict(n=512, angles=720, det=768, sod=1600.0, sdd=3200.0,
+                     pitch=1.3, ellipsoids=200, center=192.0,
+                     axes=(16.0, 160.0), seed=1234),
+    # 256^3, 360 angles, 384^2, SOD 800, SDD 1600, pitch 1.3, 40 ellipsoids
+    "config2": dict(n=256, angles=360, det=384, sod=800.0, sdd=1600.0,
+                    pitch=1.3, ellipsoids=40, center=96.0, axes=(8.0, 80.0),
+                    seed=1236),
+    # small case for profiler captures: inputs still larger than L2
+    "profile": dict(n=384, angles=128, det=576, sod=1200.0, sdd=2400.0,
+                    pitch=1.3, ellipsoids=60, center=144.0,
+                    axes=(12.0, 120.0), seed=1240),
+}
+
+
+def make_scan(w):
+    import kernelkit as kk
+
+    det = kk.Detector(rows=w["det"], cols=w["det"], pixel_height=w["pitch"],
+                      pixel_width=w["pitch"])
+    g0 = kk.ProjectionGeometry([-w["sod"], 0.0, 0.0],
+                               [w["sdd"] - w["sod"], 0.0, 0.0], det)
+    pgs = [kk.rotate(g0, yaw=2 * np.pi * k / w["angles"])
+           for k in range(w["angles"])]
+    vg = kk.resolve_volume_geometry(shape=w["n"], voxel_size=1.0)
+    return pgs, vg
+
+
+def make_volume(w, vg, device="cuda"):
+    from kernelkit import phantom
+
+    ell = phantom.random_ellipsoids(w["ellipsoids"], w["center"], w["axes"],
+                                    seed=w["seed"])
+    return phantom.voxelize_torch(ell, vg.shape, vg.extent_min,
+                                  vg.voxel_size, device=device)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons every 200 ms."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,"
+             "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(prefix="kk_clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}",
+                 f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"),
+                stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [],
+                    "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for name, val in zip(names, parts[5:9]):
+                    if val.lower() == "active":
+                        reasons.add(name)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle on a bounded sample, on all host cores
+# ---------------------------------------------------------------------------
+_SHARED = {}
+
+
+def _cpu_init(shm_name, shape):
+    from multiprocessing import shared_memory
+
+    os.environ["OMP_NUM_THREADS"] = "1"
+    shm = shared_memory.SharedMemory(name=shm_name)
+    _SHARED["shm"] = shm
+    _SHARED["vol"] = np.ndarray(shape, np.float32, buffer=shm.buf)
+
+
+def _cpu_fp_task(args):
+    from oracle import cone
+
+    p, axis, rows, cols, osc = args
+    t = time.perf_counter()
+    cone.cone_fp_angle(_SHARED["vol"], p, axis, rows, cols, osc)
+    return time.perf_counter() - t
+
+
+def _cpu_bp_task(args):
+    from oracle import cone
+
+    sino, p, shape, scale = args
+    t = time.perf_counter()
+    cone.cone_bp(sino, p, shape, scale)
+    return time.perf_counter() - t
+
+
+def cpu_sample(w, pgs, vg, vol_host, cores, fp_rows=16, bp_slab=8,
+               tasks_per_core=1):
+    """Oracle FP and BP on a bounded sample: ``fp_rows`` detector rows of
+    one angle per FP task and one angle over a ``bp_slab``-voxel slab per
+    BP task, ``cores`` tasks at a time. Returns (GUPS FP+BP, description)."""
+    import multiprocessing as mp
+    from multiprocessing import shared_memory
+
+    from kernelkit.kernels import RayDrivenConeFP, VoxelDrivenConeBP
+
+    fpar = RayDrivenConeFP.geoms2params(pgs, vg)
+    rows12 = np.stack([np.asarray(p, np.float32) for p in fpar], axis=1)
+    bpar = VoxelDrivenConeBP.geoms2params(pgs, vg).reshape(-1, 12)
+    osc = RayDrivenConeFP._output_scale(vg.voxel_size)
+    n = int(vg.shape[0])
+    det = w["det"]
+    ntasks = cores * tasks_per_core
+    idx = np.linspace(0, len(pgs) - 1, ntasks).astype(int)
+    fp_args = []
+    for k, j in enumerate(idx):
+        p = rows12[j].copy()
+        r0 = (det // 2 - fp_rows // 2)
+        p[3:6] = p[3:6] + np.float32(r0) * p[9:12]   # start at row r0
+        fp_args.append((p, int(fpar.axes[j]), fp_rows, det, osc))
+    rng = np.random.default_rng(0)
+    sino = rng.uniform(0, 1, (1, det, det)).astype(np.float32)
+    bp_args = [(sino, bpar[j:j + 1], (bp_slab, n, n), vg.voxel_volume())
+               for j in idx]
+    shm = shared_memory.SharedMemory(create=True, size=vol_host.nbytes)
+    try:
+        np.ndarray(vol_host.shape, np.float32, buffer=shm.buf)[...] = vol_host
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(cores, initializer=_cpu_init,
+                      initargs=(shm.name, vol_host.shape)) as pool:
+            t0 = time.perf_counter()
+            pool.map(_cpu_fp_task, fp_args, chunksize=1)
+            t_fp = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            pool.map(_cpu_bp_task, bp_args, chunksize=1)
+            t_bp = time.perf_counter() - t0
+    finally:
+        shm.close()
+        shm.unlink()
+    # updates covered: FP sample = fp_rows/det of one angle's N voxels
+    nvox = float(n) ** 3
+    fp_upd = ntasks * nvox * fp_rows / det
+    bp_upd = ntasks * bp_slab * float(n) * n
+    fp_rate = fp_upd / t_fp
+    bp_rate = bp_upd / t_bp
+    gups = 2.0 / (1.0 / fp_rate + 1.0 / bp_rate) / 1e9
+    desc = (f"oracle FP {ntasks} x ({fp_rows} rows x {det} cols of one angle)"
+            f" in {t_fp:.1f}s + BP {ntasks} x ({bp_slab}x{n}x{n} voxels, one "
+            f"angle) in {t_bp:.1f}s; per-update rates extrapolated to the "
+            "full workload")
+    return gups, desc, t_fp + t_bp
+
+
+# ---------------------------------------------------------------------------
+def dist_setup():
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(
+            seconds=120), device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    import torch
+
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def load_traffic(workload, kernel):
+    """DRAM bytes per launch of ``kernel`` from the committed ncu summary
+    (profiles/traffic.json), scaled to ``workload``; None if absent."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            t = json.load(f)
+        return t[workload][kernel]
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def run_ours(args):
+    import torch
+
+    from kernelkit import XrayTransform
+    from kernelkit.kernels import RayDrivenConeFP, VoxelDrivenConeBP
+
+    rank, world, local = dist_setup()
+    w = WORKLOADS[args.workload]
+    pgs, vg = make_scan(w)
+    shape = tuple(int(s) for s in vg.shape)
+    nupd = float(np.prod(shape)) * len(pgs)
+    vol = make_volume(w, vg)
+    fp = RayDrivenConeFP()
+    fp.compile()
+    fp.set_params(fp.geoms2params(pgs, vg))
+    bp = VoxelDrivenConeBP()
+    bp.compile()
+    bp.set_params(bp.geoms2params(pgs, vg))
+    proj = torch.empty((len(pgs), w["det"], w["det"]), device="cuda")
+    back = torch.empty(shape, device="cuda")
+    stream = torch.cuda.current_stream()
+    from kernelkit import _native
+
+    # the backprojector samples a layered texture of the sinogram (the
+    # reference's filter); the copy into it is part of the step
+    ptex = _native.Layered(len(pgs), w["det"], w["det"], _native.KK_F32)
+
+    def step(ev):
+        ev[0].record(stream)
+        fp(vol, pgs, vg, proj, additive=False)
+        ev[1].record(stream)
+        ptex.copy_from(proj)
+        bp(ptex, back, vg, additive=False)
+        ev[2].record(stream)
+
+    for _ in range(args.warmup):
+        step([torch.cuda.Event(enable_timing=True) for _ in range(3)])
+    barrier(world)
+    sampler = ClockSampler(local)
+    sampler.start()
+    events = [[torch.cuda.Event(enable_timing=True) for _ in range(3)]
+              for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for k in range(args.steps):
+        step(events[k])
+    t_end.record(stream)
+    barrier(world)
+    clocks = sampler.stop()
+    fp_ms = [e[0].elapsed_time(e[1]) for e in events]
+    bp_ms = [e[1].elapsed_time(e[2]) for e in events]
+    total_ms = t_start.elapsed_time(t_end)
+    ms_step = max_over_ranks(total_ms / args.steps, world)
+    t_fp = statistics.mean(fp_ms)
+    t_bp = statistics.mean(bp_ms)
+    value = world * 2 * nupd / (ms_step * 1e-3) / 1e9
+
+    e2e = None
+    if not args.no_e2e:
+        op = XrayTransform(pgs, vg)
+        host_in = torch.empty(shape, dtype=torch.float32, pin_memory=True)
+        host_in.copy_(vol.cpu())
+        host_out = torch.empty(shape, dtype=torch.float32, pin_memory=True)
+        dev_in = torch.empty(shape, device="cuda")
+        dev_y = torch.empty((len(pgs), w["det"], w["det"]), device="cuda")
+        dev_out = torch.empty(shape, device="cuda")
+
+        def e2e_step():
+            dev_in.copy_(host_in, non_blocking=True)
+            op(dev_in, out=dev_y)
+            op.T(dev_y, out=dev_out)
+            host_out.copy_(dev_out, non_blocking=True)
+
+        for _ in range(max(1, args.warmup)):
+            e2e_step()
+        barrier(world)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        b.record(stream)
+        barrier(world)
+        e2e_ms = max_over_ranks(a.elapsed_time(b) / args.steps, world)
+        e2e = {"value": world * 2 * nupd / (e2e_ms * 1e-3) / 1e9,
+               "unit": UNIT, "ms_per_step": e2e_ms,
+               "h2d_bytes_per_step": host_in.numel() * 4,
+               "d2h_bytes_per_step": host_out.numel() * 4,
+               "path": "XrayTransform: pinned host x -> A x -> A^T (A x) -> "
+                       "pinned host"}
+        del dev_in, dev_y, dev_out
+
+    peak, peak_kind = load_peaks()
+    fp_bytes = 4.0 * nupd  # algorithmic: one float32 voxel operand / update
+    roofline = {"kernel": "cone_fp_kernel", "bound": "hbm",
+                "achieved": fp_bytes / (t_fp * 1e-3) / 1e9, "peak": peak,
+                "unit": "GB/s",
+                "frac": fp_bytes / (t_fp * 1e-3) / 1e9 / peak,
+                "peak_kind": peak_kind,
+                "traffic": load_traffic(args.workload, "cone_fp_kernel"),
+                "algorithmic_bytes_per_launch": fp_bytes}
+    kernels = {
+        "cone_fp_kernel": {"ms": t_fp, "gups": nupd / (t_fp * 1e-3) / 1e9,
+                           "achieved_gbs": fp_bytes / (t_fp * 1e-3) / 1e9,
+                           "traffic": load_traffic(args.workload,
+                                                   "cone_fp_kernel")},
+        "cone_bp_kernel": {"ms": t_bp, "gups": nupd / (t_bp * 1e-3) / 1e9,
+                           "achieved_gbs": fp_bytes / (t_bp * 1e-3) / 1e9,
+                           "traffic": load_traffic(args.workload,
+                                                   "cone_bp_kernel")},
+    }
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cores = len(os.sched_getaffinity(0))
+        gups, desc, secs = cpu_sample(w, pgs, vg, vol.cpu().numpy(), cores,
+                                      fp_rows=48, bp_slab=24)
+        cpu = {"value": gups, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": desc, "seconds": secs}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "volume": list(shape),
+                       "angles": len(pgs), "detector": [w["det"], w["det"]],
+                       "sod": w["sod"], "sdd": w["sdd"], "pitch": w["pitch"],
+                       "phantom": f"{w['ellipsoids']} seeded ellipsoids",
+                       "interpolation": "texture-compatible (1/256 weights)",
+                       "l2": "inputs larger than L2 (volume 537 MB, "
+                             "sinogram 1.7 GB), no flush",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+            "kernels": kernels, "gpu_launches": 2 * args.steps,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    """Reference arm: the oracle's restatement of the reference algorithm
+    (the reference itself has no CPU path; its GPU kernels are exercised by
+    the test suite through oracle/_ref) on all host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    import torch
+
+    w = WORKLOADS[args.workload]
+    pgs, vg = make_scan(w)
+    if torch.cuda.is_available():
+        vol = make_volume(w, vg).cpu().numpy()
+    else:
+        vol = make_volume(w, vg, device="cpu").numpy()
+    cores = len(os.sched_getaffinity(0))
+    vals, descs, secs = [], None, []
+    for k in range(args.warmup + args.steps):
+        gups, descs, s = cpu_sample(w, pgs, vg, vol, cores, fp_rows=8,
+                                    bp_slab=4)
+        if k >= args.warmup:
+            vals.append(gups)
+            secs.append(s)
+    value = statistics.mean(vals)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": statistics.mean(secs) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": args.workload, "volume": [w["n"]] * 3,
+                   "angles": w["angles"], "detector": [w["det"], w["det"]]},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores,
+                         "kind": "port", "sample": descs},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS),
+                    default="headline")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

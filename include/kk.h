@@ -56,7 +56,10 @@ typedef struct {
     float u[3];        /* column step: u * pixel_width */
     float v[3];        /* row step: v * pixel_height */
     int32_t axis;      /* dominant ray axis 0/1/2 (world x/y/z) */
-    int32_t pad[3];
+    int32_t index;     /* projection (angle) this record writes; records
+                          may come in any order, e.g. interleaved by axis
+                          so every SM mixes texture and ALU work */
+    int32_t pad[2];
 } kk_fp_angle;
 
 /* Per-angle backprojection parameters: the reference's Params struct
@@ -108,6 +111,9 @@ typedef struct {
     int32_t has_max;
 } kk_bp_update;
 
+/* Opaque 2D-layered texture (see kk_layered_create below). */
+typedef struct kk_layered kk_layered;
+
 /* ---- forward projection -------------------------------------------- */
 
 /* Ray-driven cone-beam forward projection (replaces the reference's
@@ -129,21 +135,68 @@ KK_API int kk_cone_fp_residual(const kk_volume* vol, const kk_projections* out,
                                const kk_fp_residual* residual, int32_t interp,
                                int32_t slab, void* stream);
 
+/* Forward projection where rays stepping along the volume's slowest
+ * memory axis sample vtex, a kk_layered copy of the volume with one layer
+ * per slice of that axis (filled by the caller with kk_layered_copy):
+ * the texture unit then filters exactly as the reference's 3D texture
+ * does for those rays. Other rays use the device-memory path on vol.
+ * residual may be NULL (plain projection) or the SIRT epilogue. */
+KK_API int kk_cone_fp_layered(const kk_layered* vtex, const kk_volume* vol,
+                              const kk_projections* proj,
+                              const kk_fp_angle* angles,
+                              const float* out_scale,
+                              const kk_fp_residual* residual, int32_t slab,
+                              int32_t additive, void* stream);
+
 /* ---- backprojection ------------------------------------------------- */
 
 /* Voxel-driven cone-beam backprojection (replaces VoxelDrivenConeBP.__call__,
  * kernels/cone_bp.py:192-302, kernel cuda/cone_bp.cu:35-159).
  * vol = A^T proj * out_scale (additive=0) or vol += ...; out_scale is the
- * voxel volume (kernels/cone_bp.py:294). */
+ * voxel volume (kernels/cone_bp.py:294). Angles are processed in launches
+ * of 32, as the reference does, so each chunk's projections stay in L2;
+ * the running sum is kept in the volume when it is float32, otherwise in
+ * work: an optional float32 buffer with one element per voxel (dense, in
+ * the volume's memory order). With work NULL in that case one launch
+ * covers all angles (same result, more memory traffic). */
 KK_API int kk_cone_bp(const kk_projections* proj, const kk_volume* vol,
-               const kk_bp_angle* angles, float out_scale, int32_t interp,
-               int32_t additive, void* stream);
-
-/* Backprojection fused with the SIRT update epilogue (kk_bp_update). */
-KK_API int kk_cone_bp_update(const kk_projections* proj, const kk_volume* vol,
                       const kk_bp_angle* angles, float out_scale,
-                      const kk_bp_update* update, int32_t interp,
+                      int32_t interp, int32_t additive, float* work,
                       void* stream);
+
+/* Backprojection fused with the SIRT update epilogue (kk_bp_update); work
+ * as for kk_cone_bp (the update needs it whenever there are more than 32
+ * angles, to keep one launch per chunk). */
+KK_API int kk_cone_bp_update(const kk_projections* proj, const kk_volume* vol,
+                             const kk_bp_angle* angles, float out_scale,
+                             const kk_bp_update* update, int32_t interp,
+                             float* work, void* stream);
+
+/* ---- layered projection texture ---------------------------------------- */
+
+/* A 2D-layered CUDA array of the projections (one layer per angle) with a
+ * border-addressed, linearly filtered texture object: the texture the
+ * reference's BackProjector samples (projector.py:529-542, kernel.py:
+ * 91-96). Created once per scan (this is the only allocating entry
+ * point), refilled from device projections with kk_layered_copy, and
+ * sampled by kk_cone_bp_layered*, whose interpolation is then the texture
+ * unit's own. float32 or float16 texels; at most 2048 layers. */
+KK_API int kk_layered_create(int64_t layers, int64_t height, int64_t width,
+                             int32_t dtype, kk_layered** out);
+KK_API int kk_layered_copy(kk_layered* tex, const kk_projections* src,
+                           void* stream);
+KK_API int kk_layered_destroy(kk_layered* tex);
+
+/* kk_cone_bp / kk_cone_bp_update sampling the layered texture. */
+KK_API int kk_cone_bp_layered(const kk_layered* tex, const kk_volume* vol,
+                              const kk_bp_angle* angles, float out_scale,
+                              int32_t additive, float* work, void* stream);
+KK_API int kk_cone_bp_layered_update(const kk_layered* tex,
+                                     const kk_volume* vol,
+                                     const kk_bp_angle* angles,
+                                     float out_scale,
+                                     const kk_bp_update* update, float* work,
+                                     void* stream);
 
 /* ---- FDK pre-processing ---------------------------------------------- */
 

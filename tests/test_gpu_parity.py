@@ -23,8 +23,9 @@ REF_TOL = 1e-5
 ORACLE_TOL = 1e-5
 
 
-def run_fp(pgs, vg, vol, interpolation="texture"):
-    K = RayDrivenConeFP(interpolation=interpolation)
+def run_fp(pgs, vg, vol, interpolation="texture", texture_unit=True):
+    K = RayDrivenConeFP(interpolation=interpolation,
+                        use_texture_unit=texture_unit)
     K.compile()
     K.set_params(K.geoms2params(pgs, vg))
     det = pgs[0].detector
@@ -33,30 +34,35 @@ def run_fp(pgs, vg, vol, interpolation="texture"):
     return out.cpu().numpy()
 
 
-def run_bp(pgs, vg, sino, interpolation="texture"):
+def run_bp(pgs, vg, sino, interpolation="texture", fetch="global"):
     K = VoxelDrivenConeBP(interpolation=interpolation)
     K.compile()
     K.set_params(K.geoms2params(pgs, vg))
     vol = torch.zeros(tuple(int(s) for s in vg.shape), device="cuda")
-    K(torch.as_tensor(sino, device="cuda"), vol, vg)
+    src = torch.as_tensor(sino, device="cuda")
+    if fetch == "texture":  # through the layered texture (hardware filter)
+        src = kk.kernel.copy_to_texture(src, layered=True)
+    K(src, vol, vg)
     return vol.cpu().numpy()
 
 
+@pytest.mark.parametrize("texture_unit", [True, False])
 @pytest.mark.parametrize("name", GPU_CASES)
-def test_fp_matches_reference_kernel(name, gpu_golden):
+def test_fp_matches_reference_kernel(name, texture_unit, gpu_golden):
     pgs, vg = build_case(name)
-    out = run_fp(pgs, vg, case_volume(name, vg))
+    out = run_fp(pgs, vg, case_volume(name, vg), texture_unit=texture_unit)
     stride = int(gpu_golden[f"{name}/ref_fp_stride"])
     assert rel_l2(out[::stride], gpu_golden[f"{name}/ref_fp"]) <= REF_TOL
 
 
+@pytest.mark.parametrize("fetch", ["global", "texture"])
 @pytest.mark.parametrize("name", [n for n in GPU_CASES
                                   if CASES[n].get("bp", True)])
-def test_bp_matches_reference_kernel(name, gpu_golden):
+def test_bp_matches_reference_kernel(name, fetch, gpu_golden):
     pgs, vg = build_case(name)
     det = pgs[0].detector
     sino = random_sinogram(name, len(pgs), det.rows, det.cols)
-    out = run_bp(pgs, vg, sino)
+    out = run_bp(pgs, vg, sino, fetch=fetch)
     assert rel_l2(out, gpu_golden[f"{name}/ref_bp"]) <= REF_TOL
 
 

@@ -59,12 +59,14 @@ def test_bad_shapes_are_rejected():
     vol.shape[:] = (4, 4, 4)
     proj.table = 0x4000
     proj.table_axis = 1
-    rc = L.kk_cone_bp(proj, vol, ctypes.c_void_p(0x3000), 1.0, 0, 0, None)
+    rc = L.kk_cone_bp(proj, vol, ctypes.c_void_p(0x3000), 1.0, 0, 0, None,
+                      None)
     assert rc == _native.KK_ERR_UNSUPPORTED
     vol.dtype = 7
     proj.table = None
     proj.table_axis = 0
-    rc = L.kk_cone_bp(proj, vol, ctypes.c_void_p(0x3000), 1.0, 0, 0, None)
+    rc = L.kk_cone_bp(proj, vol, ctypes.c_void_p(0x3000), 1.0, 0, 0, None,
+                      None)
     assert rc == _native.KK_ERR_INVALID_ARGUMENT
 
 
