@@ -15,6 +15,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "kk_common.cuh"
 
 namespace kk {
@@ -924,4 +926,63 @@ extern "C" int kk_cone_bp_layered_update(const kk_layered* t, const kk_volume* v
         cone_bp_kernel<float, float, true, BP_UPDATE, FETCH_TEX><<<bp_grid(c), dim3(BP_TILE_2, BP_TILE_1), 0, s>>>(c);
     });
     return kk_check_launch(who);
+}
+
+// ---------------------------------------------------------------------------
+// allocation-free backprojection
+// ---------------------------------------------------------------------------
+// kk_cone_bp needs a float32 running-sum buffer (`work`) whenever the volume
+// is stored in 16 bits and there are more than 32 angles. Some callers can
+// not provide one: they cannot call cudaMalloc at all, for instance a host
+// application whose device memory is owned by a pooled allocator of its
+// own, or a program that binds only this library's C entry points and not
+// the CUDA runtime. kk_cone_bp_static serves them with a fixed buffer that
+// lives in the library itself. The buffer is a file-scope device array of
+// KK_STATIC_SCRATCH_VOXELS floats (32 MiB), so every GPU that loads the
+// library holds it until the process exits; volumes with more voxels are
+// rejected. Host code cannot use the array's name as a device address, so
+// the address is looked up once per device with cudaGetSymbolAddress.
+#define KK_STATIC_SCRATCH_VOXELS (1 << 23)
+static __device__ __align__(256) float g_bp_scratch[KK_STATIC_SCRATCH_VOXELS];
+
+#define KK_STATIC_MAX_DEVICES 64
+static float* g_bp_scratch_ptr[KK_STATIC_MAX_DEVICES];
+static std::mutex g_bp_scratch_mutex;
+
+// Device address of g_bp_scratch on the current device, looked up on the
+// first call per device (with that device current).
+static int bp_scratch_address(float** out) {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return kk_fail(KK_ERR_CUDA, "kk_cone_bp_static: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= KK_STATIC_MAX_DEVICES)
+        return kk_fail(KK_ERR_UNSUPPORTED, "kk_cone_bp_static: device %d beyond %d", dev, KK_STATIC_MAX_DEVICES);
+    std::lock_guard<std::mutex> lock(g_bp_scratch_mutex);
+    if (!g_bp_scratch_ptr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_bp_scratch);
+        if (e != cudaSuccess || !p)
+            return kk_fail(KK_ERR_CUDA, "kk_cone_bp_static: cudaGetSymbolAddress failed: %s",
+                           cudaGetErrorString(e));
+        g_bp_scratch_ptr[dev] = (float*)p;
+    }
+    *out = g_bp_scratch_ptr[dev];
+    return KK_OK;
+}
+
+extern "C" int kk_cone_bp_static(const kk_projections* proj, const kk_volume* vol, const kk_bp_angle* angles,
+                                 float out_scale, int32_t interp, int32_t additive, void* stream) {
+    if (vol && vol->shape[0] > 0 && vol->shape[1] > 0 && vol->shape[2] > 0 &&
+        vol->shape[0] * vol->shape[1] * vol->shape[2] > (int64_t)KK_STATIC_SCRATCH_VOXELS)
+        return kk_fail(KK_ERR_INVALID_ARGUMENT,
+                       "kk_cone_bp_static: %lld voxels exceed the built-in buffer of %d voxels; "
+                       "use kk_cone_bp with a caller-provided work buffer",
+                       (long long)(vol->shape[0] * vol->shape[1] * vol->shape[2]), KK_STATIC_SCRATCH_VOXELS);
+    float* scratch = nullptr;
+    int rc = bp_scratch_address(&scratch);
+    if (rc) return rc;
+    // every chunk after the first reads back what the previous chunk of the
+    // same call wrote, and the first chunk starts from zero or the volume,
+    // so the buffer's previous contents never matter
+    return kk_cone_bp(proj, vol, angles, out_scale, interp, additive, scratch, stream);
 }

@@ -61,7 +61,7 @@ BP_ANGLE_DTYPE = np.dtype([("num_u", "<f4", 4), ("num_v", "<f4", 4),
 
 #: every symbol include/kk.h declares
 EXPORTS = ("kk_cone_fp", "kk_cone_fp_residual", "kk_cone_fp_layered",
-           "kk_cone_bp",
+           "kk_cone_bp", "kk_cone_bp_static",
            "kk_cone_bp_update", "kk_layered_create", "kk_layered_copy",
            "kk_layered_destroy", "kk_cone_bp_layered",
            "kk_cone_bp_layered_update", "kk_preweight", "kk_filter_rows",
@@ -97,6 +97,8 @@ def load():
                              i32, vp, vp]
     L.kk_cone_bp_update.argtypes = [P(kk_projections), P(kk_volume), vp, f32,
                                     P(kk_bp_update), i32, vp, vp]
+    L.kk_cone_bp_static.argtypes = [P(kk_projections), P(kk_volume), vp, f32,
+                                    i32, i32, vp]
     L.kk_layered_create.argtypes = [i64, i64, i64, i32, P(vp)]
     L.kk_layered_copy.argtypes = [vp, P(kk_projections), vp]
     L.kk_layered_destroy.argtypes = [vp]
