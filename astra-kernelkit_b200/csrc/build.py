@@ -18,7 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(os.path.dirname(HERE), "kernelkit")
 INCLUDE = os.path.join(os.path.dirname(os.path.dirname(HERE)), "include")
 OUT = os.path.join(PKG, "_native", "libkk.so")
-SOURCES = ["kk_capi.cu", "kk_cone.cu", "kk_fdk.cu"]
+SOURCES = ["kk_capi.cu", "kk_fp.cu", "kk_bp.cu", "kk_fdk.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
                 "-Xcompiler", "-fvisibility=hidden", f"-I{INCLUDE}", f"-I{HERE}"]
@@ -49,15 +49,18 @@ def build(verbose: bool = False, force: bool = False, extra=(),
     os.makedirs(os.path.dirname(out), exist_ok=True)
     tmp = tempfile.mkdtemp(prefix="kk_build_")
     try:
-        objs = []
-        for src in SOURCES:
+        objs, procs = [], []
+        for src in SOURCES:  # translation units compile in parallel
             obj = os.path.join(tmp, src.replace(".cu", ".o"))
             cmd = [nvcc(), *FLAGS, *extra, "-c", os.path.join(HERE, src),
                    "-o", obj]
             if verbose:
                 print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
+            procs.append((cmd, subprocess.Popen(cmd)))
             objs.append(obj)
+        for cmd, p in procs:
+            if p.wait() != 0:
+                raise subprocess.CalledProcessError(p.returncode, cmd)
         lib = os.path.join(tmp, "libkk.so")
         subprocess.run([nvcc(), *ARCH, "-shared", *objs, "-o", lib,
                         "-lcudart"], check=True)

@@ -1,0 +1,450 @@
+// Cone-beam backprojection (voxel-driven) for sm_100a: kernel, layered
+// projection textures and the kk_cone_bp* entry points of include/kk.h.
+#include <mutex>
+
+#include "kk_cone.cuh"
+
+namespace kk {
+
+// ---------------------------------------------------------------------------
+// backprojection: one thread per (fast, middle) voxel column and a group of
+// BP_GROUP voxels along the slowest memory axis
+// ---------------------------------------------------------------------------
+template <typename TP, typename TV, bool TEX8, int EPI, int FETCH>
+__global__ void __launch_bounds__(BP_TILE_2* BP_TILE_1) cone_bp_kernel(const BpArgs L) {
+    // One launch covers the angles [j_begin, j_end): one 32-angle chunk,
+    // as one launch of the reference does (kernels/cone_bp.py:297-302), so
+    // the chunk's projections stay in L2 while every voxel reads them; the
+    // running sum vol += acc * scale is carried between launches in the
+    // volume (float32) or in the float32 work buffer.
+    __shared__ kk_bp_angle sp[BP_CHUNK];
+    const int i2 = blockIdx.x * BP_TILE_2 + threadIdx.x;
+    const int i1 = blockIdx.y * BP_TILE_1 + threadIdx.y;
+    const int g0 = blockIdx.z * BP_GROUP;
+    const int n0 = L.vn[L.m0], n1 = L.vn[L.m1], n2 = L.vn[L.m2];
+    const bool active = i2 < n2 && i1 < n1;
+    const int cnt = min(BP_GROUP, n0 - g0);
+
+    // centre of the group's first voxel, world axes
+    float f[3];
+    f[L.m0] = __fadd_rn(__fsub_rn((float)g0, 0.5f * (float)n0), 0.5f);
+    f[L.m1] = __fadd_rn(__fsub_rn((float)i1, 0.5f * (float)n1), 0.5f);
+    f[L.m2] = __fadd_rn(__fsub_rn((float)i2, 0.5f * (float)n2), 0.5f);
+    const float X = f[0], Y = f[1], Z = f[2];
+    const int m0 = L.m0;
+
+    TV* vol = (TV*)L.vol;
+    const int64_t vbase = (int64_t)g0 * L.vs[L.m0] + (int64_t)i1 * L.vs[L.m1] + (int64_t)i2 * L.vs[L.m2];
+    const int64_t vstep = L.vs[L.m0];
+    // the work buffer is dense in the volume's memory order
+    const int64_t wbase = ((int64_t)g0 * n1 + i1) * n2 + i2;
+    const int64_t wstep = (int64_t)n1 * n2;
+
+    float acc[BP_GROUP], vacc[BP_GROUP];
+#pragma unroll
+    for (int i = 0; i < BP_GROUP; ++i) {
+        acc[i] = 0.f;
+        vacc[i] = 0.f;
+        if (active && i < cnt) {
+            if (L.load_mode == LOAD_VOL)
+                vacc[i] = ld_rw(vol + vbase + i * vstep);
+            else if (L.load_mode == LOAD_WORK)
+                vacc[i] = L.work[wbase + i * wstep];
+        }
+    }
+
+    const int tid = threadIdx.y * BP_TILE_2 + threadIdx.x;
+    for (int j0 = L.j_begin; j0 < L.j_end; j0 += BP_CHUNK) {
+        const int nj = min(BP_CHUNK, L.j_end - j0);
+        __syncthreads();
+        for (int k = tid; k < nj * 12; k += BP_TILE_2 * BP_TILE_1)
+            ((float*)sp)[k] = __ldg((const float*)(L.angles + j0) + k);
+        __syncthreads();
+        if (!active) continue;
+        for (int jj = 0; jj < nj; ++jj) {
+            const kk_bp_angle& q = sp[jj];
+            const int j = j0 + jj;
+            const TP* plane = FETCH == FETCH_TEX ? nullptr
+                              : (L.table ? (const TP*)L.table[j] : (const TP*)L.proj + (int64_t)j * L.ps[0]);
+            float nu = fmaf(Z, q.num_u[2], fmaf(Y, q.num_u[1], fmaf(X, q.num_u[0], q.num_u[3])));
+            float nv = fmaf(Z, q.num_v[2], fmaf(Y, q.num_v[1], fmaf(X, q.num_v[0], q.num_v[3])));
+            float dn = fmaf(Z, q.den[2], fmaf(Y, q.den[1], fmaf(X, q.den[0], q.den[3])));
+            const float du = q.num_u[m0], dv = q.num_v[m0], dd = q.den[m0];
+#pragma unroll
+            for (int i = 0; i < BP_GROUP; ++i) {
+                if (i < cnt) {
+                    const float rr = __fdividef(1.f, dn);
+                    const float U = __fmul_rn(nu, rr);
+                    const float V = __fmul_rn(nv, rr);
+                    float val;
+                    if (FETCH == FETCH_TEX)  // the hardware filter the reference samples with
+                        val = tex2DLayered<float>(L.tex, U, V, j);
+                    else
+                        val = bilinear<TEX8>(plane, L.ps[1], L.ps[2], L.rows, L.cols, V, U);
+                    acc[i] = fmaf(__fmul_rn(rr, rr), val, acc[i]);
+                }
+                nu = __fadd_rn(nu, du);
+                nv = __fadd_rn(nv, dv);
+                dn = __fadd_rn(dn, dd);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < BP_GROUP; ++i) {
+            vacc[i] = fmaf(acc[i], L.scale, vacc[i]);
+            acc[i] = 0.f;
+        }
+    }
+    if (!active) return;
+#pragma unroll
+    for (int i = 0; i < BP_GROUP; ++i) {
+        if (i >= cnt) break;
+        TV* p = vol + vbase + i * vstep;
+        if (L.store_mode == STORE_WORK) {
+            L.work[wbase + i * wstep] = vacc[i];
+        } else if (EPI == BP_UPDATE) {
+            const int64_t e = vbase + i * vstep;
+            float x = ld_rw(p);
+            x = __fsub_rn(x, __fmul_rn(vacc[i], __ldg(L.upd_scale + e)));
+            if (L.upd_mask) x = __fmul_rn(x, __ldg(L.upd_mask + e));
+            if (L.has_min) x = fmaxf(x, L.vmin);
+            if (L.has_max) x = fminf(x, L.vmax);
+            st(p, x);
+        } else {
+            st(p, vacc[i]);
+        }
+    }
+}
+
+}  // namespace kk
+
+// ===========================================================================
+// host side
+// ===========================================================================
+using namespace kk;
+
+// ---------------------------------------------------------------------------
+
+static dim3 bp_grid(const BpArgs& L) {
+    return dim3((L.vn[L.m2] + BP_TILE_2 - 1) / BP_TILE_2, (L.vn[L.m1] + BP_TILE_1 - 1) / BP_TILE_1,
+                (L.vn[L.m0] + BP_GROUP - 1) / BP_GROUP);
+}
+
+template <typename TP, typename TV, int EPI>
+static void launch_bp_typed(const BpArgs& L, bool tex8, cudaStream_t s) {
+    dim3 block(BP_TILE_2, BP_TILE_1);
+    if (tex8)
+        cone_bp_kernel<TP, TV, true, EPI, FETCH_GLOBAL><<<bp_grid(L), block, 0, s>>>(L);
+    else
+        cone_bp_kernel<TP, TV, false, EPI, FETCH_GLOBAL><<<bp_grid(L), block, 0, s>>>(L);
+}
+
+// Launch `one` once per 32-angle chunk. The running sum lives in the volume
+// when it is float32 and the result is a plain sum; otherwise in the
+// float32 work buffer (when given). Without a buffer in those cases a
+// single launch covers every angle (same arithmetic, more L2 traffic).
+template <typename Fn>
+static void bp_chunks(BpArgs L, bool vol_f32, bool additive, bool update, Fn one) {
+    const int n = L.n_angles;
+    const int chunks = (n + BP_CHUNK - 1) / BP_CHUNK;
+    const bool need_work = chunks > 1 && (!vol_f32 || update);
+    const int first_load = (additive && !update) ? LOAD_VOL : LOAD_ZERO;
+    if (need_work && !L.work) {
+        L.j_begin = 0;
+        L.j_end = n;
+        L.load_mode = first_load;
+        L.store_mode = STORE_FINAL;
+        one(L);
+        return;
+    }
+    for (int c = 0; c < chunks; ++c) {
+        L.j_begin = c * BP_CHUNK;
+        L.j_end = min(n, L.j_begin + BP_CHUNK);
+        L.load_mode = c == 0 ? first_load : (need_work ? LOAD_WORK : LOAD_VOL);
+        L.store_mode = c == chunks - 1 ? STORE_FINAL : (need_work ? STORE_WORK : STORE_VOL);
+        one(L);
+    }
+}
+
+template <int EPI>
+static int launch_bp(const BpArgs& L, int pdt, int vdt, bool tex8, bool additive, cudaStream_t s) {
+#define KK_BP_CASE(PD, VD, TP, TV)                                                                  \
+    if (pdt == PD && vdt == VD) {                                                                   \
+        bp_chunks(L, VD == KK_F32, additive, EPI == BP_UPDATE,                                      \
+                  [&](const BpArgs& c) { launch_bp_typed<TP, TV, EPI>(c, tex8, s); });             \
+        return kk_check_launch("kk_cone_bp");                                                      \
+    }
+    KK_BP_CASE(KK_F32, KK_F32, float, float)
+    if (EPI == BP_STORE) {
+        KK_BP_CASE(KK_F16, KK_F32, __half, float)
+        KK_BP_CASE(KK_BF16, KK_F32, __nv_bfloat16, float)
+        KK_BP_CASE(KK_F16, KK_BF16, __half, __nv_bfloat16)
+        KK_BP_CASE(KK_F16, KK_F16, __half, __half)
+        KK_BP_CASE(KK_BF16, KK_BF16, __nv_bfloat16, __nv_bfloat16)
+        KK_BP_CASE(KK_F32, KK_BF16, float, __nv_bfloat16)
+        KK_BP_CASE(KK_F32, KK_F16, float, __half)
+    }
+#undef KK_BP_CASE
+    return kk_fail(KK_ERR_UNSUPPORTED, "kk_cone_bp: dtype combination projections=%d volume=%d", pdt, vdt);
+}
+
+static int fill_bp_args(BpArgs& L, const kk_projections* proj, const kk_volume* vol, const kk_bp_angle* angles,
+                        float out_scale, int32_t interp, const char* who) {
+    int rc = check_volume(vol, who);
+    if (rc) return rc;
+    rc = check_projections(proj, who);
+    if (rc) return rc;
+    if (!angles) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: angle parameters are NULL", who);
+    if (interp != KK_INTERP_TEX8 && interp != KK_INTERP_EXACT)
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: unknown interpolation mode %d", who, interp);
+    L = BpArgs{};
+    L.proj = proj->data;
+    L.table = proj->table;
+    for (int k = 0; k < 3; ++k) {
+        L.ps[k] = proj->stride[k];
+        L.vs[k] = vol->stride[k];
+        L.vn[k] = (int)vol->shape[k];
+    }
+    L.n_angles = (int)proj->n_angles;
+    L.rows = (int)proj->rows;
+    L.cols = (int)proj->cols;
+    L.vol = vol->data;
+    L.angles = angles;
+    L.scale = out_scale;
+    // memory order of the world axes: the largest stride is the slowest
+    // axis, the one the reference's threads step along (cone_bp.cu:148-151)
+    int ord[3] = {0, 1, 2};
+    for (int i = 0; i < 3; ++i)
+        for (int j = i + 1; j < 3; ++j)
+            if (vol->stride[ord[j]] > vol->stride[ord[i]]) {
+                int t = ord[i];
+                ord[i] = ord[j];
+                ord[j] = t;
+            }
+    L.m0 = ord[0];
+    L.m1 = ord[1];
+    L.m2 = ord[2];
+    if ((vol->shape[L.m1] + BP_TILE_1 - 1) / BP_TILE_1 > MAX_GRID_Y ||
+        (vol->shape[L.m0] + BP_GROUP - 1) / BP_GROUP > MAX_GRID_Y)
+        return kk_fail(KK_ERR_UNSUPPORTED, "%s: volume too large for one launch", who);
+    return KK_OK;
+}
+
+extern "C" int kk_cone_bp(const kk_projections* proj, const kk_volume* vol, const kk_bp_angle* angles,
+                          float out_scale, int32_t interp, int32_t additive, float* work, void* stream) {
+    BpArgs L;
+    int rc = fill_bp_args(L, proj, vol, angles, out_scale, interp, "kk_cone_bp");
+    if (rc) return rc;
+    L.work = work;
+    return launch_bp<BP_STORE>(L, proj->dtype, vol->dtype, interp == KK_INTERP_TEX8, additive != 0,
+                               (cudaStream_t)stream);
+}
+
+extern "C" int kk_cone_bp_update(const kk_projections* proj, const kk_volume* vol, const kk_bp_angle* angles,
+                                 float out_scale, const kk_bp_update* update, int32_t interp, float* work,
+                                 void* stream) {
+    BpArgs L;
+    int rc = fill_bp_args(L, proj, vol, angles, out_scale, interp, "kk_cone_bp_update");
+    if (rc) return rc;
+    if (!update || !update->scale)
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_cone_bp_update: update scale is NULL");
+    if (proj->dtype != KK_F32 || vol->dtype != KK_F32)
+        return kk_fail(KK_ERR_UNSUPPORTED, "kk_cone_bp_update: float32 volume and projections only");
+    L.upd_scale = update->scale;
+    L.upd_mask = update->mask;
+    L.vmin = update->min_value;
+    L.vmax = update->max_value;
+    L.has_min = update->has_min;
+    L.has_max = update->has_max;
+    L.work = work;
+    return launch_bp<BP_UPDATE>(L, proj->dtype, vol->dtype, interp == KK_INTERP_TEX8, false, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+// layered texture of the projections (reference: the 2D-layered CUDA array
+// BackProjector samples with, projector.py:529-542 and kernel.py:91-96)
+// ---------------------------------------------------------------------------
+
+extern "C" int kk_layered_create(int64_t layers, int64_t height, int64_t width, int32_t dtype, kk_layered** out) {
+    if (!out) return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_layered_create: out is NULL");
+    *out = nullptr;
+    if (layers <= 0 || height <= 0 || width <= 0 || layers > 2048 || height >= (int64_t)COORD_LIMIT ||
+        width >= (int64_t)COORD_LIMIT)
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_layered_create: bad extent (%lld, %lld, %lld)",
+                       (long long)layers, (long long)height, (long long)width);
+    if (dtype != KK_F32 && dtype != KK_F16)
+        return kk_fail(KK_ERR_UNSUPPORTED, "kk_layered_create: float32 or float16 texels only");
+    cudaChannelFormatDesc ch = dtype == KK_F32 ? cudaCreateChannelDesc<float>() : cudaCreateChannelDescHalf();
+    kk_layered* t = new kk_layered();
+    t->layers = layers;
+    t->height = height;
+    t->width = width;
+    t->dtype = dtype;
+    cudaError_t e = cudaMalloc3DArray(&t->array, &ch, make_cudaExtent(width, height, layers), cudaArrayLayered);
+    if (e != cudaSuccess) {
+        delete t;
+        return kk_fail(KK_ERR_CUDA, "kk_layered_create: %s", cudaGetErrorString(e));
+    }
+    cudaResourceDesc rd = {};
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = t->array;
+    cudaTextureDesc td = {};
+    td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeBorder;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    e = cudaCreateTextureObject(&t->tex, &rd, &td, nullptr);
+    if (e != cudaSuccess) {
+        cudaFreeArray(t->array);
+        delete t;
+        return kk_fail(KK_ERR_CUDA, "kk_layered_create: %s", cudaGetErrorString(e));
+    }
+    *out = t;
+    return KK_OK;
+}
+
+extern "C" int kk_layered_destroy(kk_layered* t) {
+    if (!t) return KK_OK;
+    cudaDestroyTextureObject(t->tex);
+    cudaFreeArray(t->array);
+    delete t;
+    return KK_OK;
+}
+
+extern "C" int kk_layered_copy(kk_layered* t, const kk_projections* src, void* stream) {
+    if (!t || !src) return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_layered_copy: NULL argument");
+    if (src->table || !src->data)
+        return kk_fail(KK_ERR_UNSUPPORTED, "kk_layered_copy: strided projections only");
+    if (src->n_angles != t->layers || src->rows != t->height || src->cols != t->width || src->dtype != t->dtype)
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_layered_copy: shape or dtype differs from the texture");
+    const size_t es = t->dtype == KK_F32 ? 4 : 2;
+    if (src->stride[2] != 1 || src->stride[0] != src->rows * src->stride[1])
+        return kk_fail(KK_ERR_UNSUPPORTED, "kk_layered_copy: rows must be contiguous and angles dense");
+    cudaMemcpy3DParms cp = {};
+    cp.srcPtr = make_cudaPitchedPtr(src->data, (size_t)src->stride[1] * es, (size_t)src->cols, (size_t)src->rows);
+    cp.dstArray = t->array;
+    cp.extent = make_cudaExtent(t->width, t->height, t->layers);
+    cp.kind = cudaMemcpyDeviceToDevice;
+    cudaError_t e = cudaMemcpy3DAsync(&cp, (cudaStream_t)stream);
+    if (e != cudaSuccess) return kk_fail(KK_ERR_CUDA, "kk_layered_copy: %s", cudaGetErrorString(e));
+    return KK_OK;
+}
+
+static int layered_args(BpArgs& L, const kk_layered* t, const kk_volume* vol, const kk_bp_angle* angles,
+                        float out_scale, const char* who) {
+    if (!t) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: texture is NULL", who);
+    kk_projections p = {};
+    p.data = (void*)1;  // texels come from the texture; the descriptor carries the extent
+    p.n_angles = t->layers;
+    p.rows = t->height;
+    p.cols = t->width;
+    p.stride[0] = t->height * t->width;
+    p.stride[1] = t->width;
+    p.stride[2] = 1;
+    p.dtype = KK_F32;
+    int rc = fill_bp_args(L, &p, vol, angles, out_scale, KK_INTERP_TEX8, who);
+    if (rc) return rc;
+    L.proj = nullptr;
+    L.tex = t->tex;
+    return KK_OK;
+}
+
+extern "C" int kk_cone_bp_layered(const kk_layered* t, const kk_volume* vol, const kk_bp_angle* angles,
+                                  float out_scale, int32_t additive, float* work, void* stream) {
+    BpArgs L;
+    int rc = layered_args(L, t, vol, angles, out_scale, "kk_cone_bp_layered");
+    if (rc) return rc;
+    L.work = work;
+    const dim3 block(BP_TILE_2, BP_TILE_1);
+    const cudaStream_t s = (cudaStream_t)stream;
+    const int vdt = vol->dtype;
+    bp_chunks(L, vdt == KK_F32, additive != 0, false, [&](const BpArgs& c) {
+        if (vdt == KK_F32)
+            cone_bp_kernel<float, float, true, BP_STORE, FETCH_TEX><<<bp_grid(c), block, 0, s>>>(c);
+        else if (vdt == KK_BF16)
+            cone_bp_kernel<float, __nv_bfloat16, true, BP_STORE, FETCH_TEX><<<bp_grid(c), block, 0, s>>>(c);
+        else
+            cone_bp_kernel<float, __half, true, BP_STORE, FETCH_TEX><<<bp_grid(c), block, 0, s>>>(c);
+    });
+    return kk_check_launch("kk_cone_bp_layered");
+}
+
+extern "C" int kk_cone_bp_layered_update(const kk_layered* t, const kk_volume* vol, const kk_bp_angle* angles,
+                                         float out_scale, const kk_bp_update* update, float* work, void* stream) {
+    const char* who = "kk_cone_bp_layered_update";
+    if (!update || !update->scale) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: update scale is NULL", who);
+    if (!vol || vol->dtype != KK_F32) return kk_fail(KK_ERR_UNSUPPORTED, "%s: float32 volume only", who);
+    BpArgs L;
+    int rc = layered_args(L, t, vol, angles, out_scale, who);
+    if (rc) return rc;
+    L.upd_scale = update->scale;
+    L.upd_mask = update->mask;
+    L.vmin = update->min_value;
+    L.vmax = update->max_value;
+    L.has_min = update->has_min;
+    L.has_max = update->has_max;
+    L.work = work;
+    const cudaStream_t s = (cudaStream_t)stream;
+    bp_chunks(L, true, false, true, [&](const BpArgs& c) {
+        cone_bp_kernel<float, float, true, BP_UPDATE, FETCH_TEX><<<bp_grid(c), dim3(BP_TILE_2, BP_TILE_1), 0, s>>>(c);
+    });
+    return kk_check_launch(who);
+}
+
+// ---------------------------------------------------------------------------
+// allocation-free backprojection
+// ---------------------------------------------------------------------------
+// kk_cone_bp needs a float32 running-sum buffer (`work`) whenever the volume
+// is stored in 16 bits and there are more than 32 angles. Some callers can
+// not provide one: they cannot call cudaMalloc at all, for instance a host
+// application whose device memory is owned by a pooled allocator of its
+// own, or a program that binds only this library's C entry points and not
+// the CUDA runtime. kk_cone_bp_static serves them with a fixed buffer that
+// lives in the library itself. The buffer is a file-scope device array of
+// KK_STATIC_SCRATCH_VOXELS floats (32 MiB), so every GPU that loads the
+// library holds it until the process exits; volumes with more voxels are
+// rejected. Host code cannot use the array's name as a device address, so
+// the address is looked up once per device with cudaGetSymbolAddress.
+#define KK_STATIC_SCRATCH_VOXELS (1 << 23)
+static __device__ __align__(256) float g_bp_scratch[KK_STATIC_SCRATCH_VOXELS];
+
+#define KK_STATIC_MAX_DEVICES 64
+static float* g_bp_scratch_ptr[KK_STATIC_MAX_DEVICES];
+static std::mutex g_bp_scratch_mutex;
+
+// Device address of g_bp_scratch on the current device, looked up on the
+// first call per device (with that device current).
+static int bp_scratch_address(float** out) {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return kk_fail(KK_ERR_CUDA, "kk_cone_bp_static: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= KK_STATIC_MAX_DEVICES)
+        return kk_fail(KK_ERR_UNSUPPORTED, "kk_cone_bp_static: device %d beyond %d", dev, KK_STATIC_MAX_DEVICES);
+    std::lock_guard<std::mutex> lock(g_bp_scratch_mutex);
+    if (!g_bp_scratch_ptr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_bp_scratch);
+        if (e != cudaSuccess || !p)
+            return kk_fail(KK_ERR_CUDA, "kk_cone_bp_static: cudaGetSymbolAddress failed: %s",
+                           cudaGetErrorString(e));
+        g_bp_scratch_ptr[dev] = (float*)p;
+    }
+    *out = g_bp_scratch_ptr[dev];
+    return KK_OK;
+}
+
+extern "C" int kk_cone_bp_static(const kk_projections* proj, const kk_volume* vol, const kk_bp_angle* angles,
+                                 float out_scale, int32_t interp, int32_t additive, void* stream) {
+    if (vol && vol->shape[0] > 0 && vol->shape[1] > 0 && vol->shape[2] > 0 &&
+        vol->shape[0] * vol->shape[1] * vol->shape[2] > (int64_t)KK_STATIC_SCRATCH_VOXELS)
+        return kk_fail(KK_ERR_INVALID_ARGUMENT,
+                       "kk_cone_bp_static: %lld voxels exceed the built-in buffer of %d voxels; "
+                       "use kk_cone_bp with a caller-provided work buffer",
+                       (long long)(vol->shape[0] * vol->shape[1] * vol->shape[2]), KK_STATIC_SCRATCH_VOXELS);
+    float* scratch = nullptr;
+    int rc = bp_scratch_address(&scratch);
+    if (rc) return rc;
+    // every chunk after the first reads back what the previous chunk of the
+    // same call wrote, and the first chunk starts from zero or the volume,
+    // so the buffer's previous contents never matter
+    return kk_cone_bp(proj, vol, angles, out_scale, interp, additive, scratch, stream);
+}

@@ -49,6 +49,28 @@ template <>
 __device__ __forceinline__ void st<__half>(__half* p, float v) { *p = __float2half_rn(v); }
 
 // ---------------------------------------------------------------------------
+// paired float32 arithmetic (sm_100 FADD2/FMUL2/FFMA2): one instruction
+// performs the same IEEE operation on two independent lanes, bit for bit
+// what two scalar instructions with the same rounding would give
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 add2_rd(float2 a, float2 b) { return __fadd2_rd(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 fma2_rd(float2 a, float2 b, float2 c) { return __ffma2_rd(a, b, c); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+    unsigned long long ra, rb, rd;
+    memcpy(&ra, &a, 8);
+    memcpy(&rb, &b, 8);
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(rd) : "l"(ra), "l"(rb));
+    float2 d;
+    memcpy(&d, &rd, 8);
+    return d;
+}
+
+// ---------------------------------------------------------------------------
 // interpolation weights
 // ---------------------------------------------------------------------------
 // CUDA's linear texture filtering (unnormalised coordinates, border

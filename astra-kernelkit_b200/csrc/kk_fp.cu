@@ -1,0 +1,510 @@
+// Cone-beam forward projection (ray-driven) for sm_100a: kernel and the
+// kk_cone_fp* entry points of include/kk.h.
+#include "kk_cone.cuh"
+
+namespace kk {
+
+// ---------------------------------------------------------------------------
+// forward projection
+// ---------------------------------------------------------------------------
+// Block = one angle, FP_COLS detector columns (one per warp) x FP_ROWS_T
+// rows; lane l of warp w traces rows r0 + l + 32 k (k < FP_RPT) of column
+// c0 + w, so a warp's loads for one slice cover consecutive rows, i.e.
+// consecutive positions along the fastest volume axis in the usual layout.
+// Blocks are ordered (row tile, angle, column tile) with the row tile
+// slowest: for circular scans about z the rows of a tile see one z-slab of
+// the volume, which then stays in L2 while every angle projects it.
+//
+// Three code paths, chosen per block: the ray's second in-slice axis D2 is
+// the unit-stride axis (FAST) and, in addition, the detector's v vector has
+// no component along the ray axis and D1 (SHARED): then every row of a
+// column sees the same D1 coordinate sequence, bit for bit, and the D1
+// split is done once per slice for the thread's rows. Otherwise a generic
+// per-ray path with arbitrary strides is used.
+#ifndef KK_FP_RPT
+#define KK_FP_RPT 2
+#endif
+#ifndef KK_FP_MINBLOCKS
+#define KK_FP_MINBLOCKS 6
+#endif
+#ifndef KK_FP_UNROLL
+#define KK_FP_UNROLL 4  // slices per unrolled step of the unchecked loops
+#endif
+constexpr int FP_RPT = KK_FP_RPT;       // rays per thread
+constexpr int FP_UNROLL = KK_FP_UNROLL;
+constexpr int FP_COLS = 8;              // columns per block (one per warp)
+constexpr int FP_ROWS_T = 32 * FP_RPT;  // rows per block
+
+struct RaySetup {
+    float a1, a2, b1, b2, corr;
+};
+
+// Per-ray slopes/offsets with the reference's float32 operation sequence
+// (cuda/cone_fp.cu:150-170, 197).
+__device__ __forceinline__ RaySetup ray_setup(const float* src, const float* cor, const float* u, const float* v,
+                                              int A, int D1, int D2, int r, int c, float sc1, float sc2) {
+    float det[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float ds = __fadd_rn(__fadd_rn(cor[k], __fmul_rn(0.5f, u[k])), __fmul_rn(0.5f, v[k]));
+        det[k] = fmaf((float)r, v[k], fmaf((float)c, u[k], ds));
+    }
+    RaySetup R;
+    const float sA = pick3(src, A), s1 = pick3(src, D1), s2 = pick3(src, D2);
+    const float sdd = __fsub_rn(sA, pick3(det, A));
+    R.a1 = __fdiv_rn(__fsub_rn(s1, pick3(det, D1)), sdd);
+    R.a2 = __fdiv_rn(__fsub_rn(s2, pick3(det, D2)), sdd);
+    R.b1 = fmaf(-R.a1, sA, s1);
+    R.b2 = fmaf(-R.a2, sA, s2);
+    R.corr = __fsqrt_rn(__fadd_rn(fmaf(__fmul_rn(R.a1, R.a1), sc1, __fmul_rn(__fmul_rn(R.a2, R.a2), sc2)), 1.f));
+    return R;
+}
+
+// Bilinear sample times weight_unit() on a plane whose D2 axis has unit
+// stride, in the unified form of the texture rules: with F, S the weights
+// along the fast (D2) and slow (D1) axes and y = F S / 256,
+//   256 v = 256 t00 + S (t01 - t00) + x1 (t11 - t01) + x0 (t10 - t00)
+// with t[fast][slow], and (x1, x0) = (h, F - h) for rule 0, (h, F - d) for
+// rule 1 (h, d = y rounded half up / half down). Added into acc.
+// CHECKED: border texels read zero and the coordinate is clamped;
+// otherwise the caller guarantees all four texels lie inside the volume.
+template <bool TEX8, bool CHECKED, int RULE, typename T>
+__device__ __forceinline__ float fast_sample(float acc, const T* __restrict__ row0, const T* __restrict__ row1,
+                                             bool y0ok, bool y1ok, int n2, float S, float zc) {
+    const Split b = CHECKED ? split_coord<TEX8>(zc) : split_unclamped<TEX8>(zc);
+    float t00, t10, t01, t11;
+    if (CHECKED) {
+        const bool z0ok = (unsigned)b.i < (unsigned)n2;
+        const bool z1ok = (unsigned)(b.i + 1) < (unsigned)n2;
+        t00 = (y0ok && z0ok) ? ld(row0 + b.i) : 0.f;      // fast 0, slow 0
+        t10 = (y0ok && z1ok) ? ld(row0 + b.i + 1) : 0.f;  // fast 1, slow 0
+        t01 = (y1ok && z0ok) ? ld(row1 + b.i) : 0.f;      // fast 0, slow 1
+        t11 = (y1ok && z1ok) ? ld(row1 + b.i + 1) : 0.f;
+    } else {
+        t00 = ld(row0 + b.i);
+        t10 = ld(row0 + b.i + 1);
+        t01 = ld(row1 + b.i);
+        t11 = ld(row1 + b.i + 1);
+    }
+    const float F = b.w;
+    float x1, x0;
+    if (TEX8) {
+        const float yy = F * S * (1.f / 256.f);  // exact
+        x1 = __fadd_rd(yy + 0.5f, 12582912.f) - 12582912.f;  // round half up
+        if (RULE == 1) {
+            const float d = -(__fadd_rd(0.5f - yy, 12582912.f) - 12582912.f);  // round half down
+            x0 = F - d;
+        } else {
+            x0 = F - x1;
+        }
+    } else {
+        x1 = F * S;
+        x0 = F - x1;
+    }
+    acc = fmaf(weight_unit<TEX8>(), t00, acc);
+    acc = fmaf(S, t01 - t00, acc);
+    acc = fmaf(x1, t11 - t01, acc);
+    acc = fmaf(x0, t10 - t00, acc);
+    return acc;
+}
+
+// Slab classification of a ray from its coordinates at the first and last
+// slice of the slab (coordinates move linearly; the float32 increments
+// drift by far less than the margins). 2 = both texels of every sample
+// inside the array, 0 = every sample reads only border zeros, 1 = mixed.
+__device__ __forceinline__ int span_class(float c0, float c1, int n) {
+    const float lo = fminf(c0, c1), hi = fmaxf(c0, c1);
+    // texel i = floor(x - 1/2) on the 1/256 grid: i >= 0 iff x >= 0.498,
+    // i + 1 <= n - 1 iff x < n - 0.502; both out iff x < -0.502 or
+    // x >= n + 0.498
+    if (lo >= 0.53f && hi <= (float)n - 0.53f) return 2;
+    if (hi < -0.53f || lo > (float)n + 0.53f) return 0;
+    return 1;
+}
+
+template <typename TV, typename TP, bool TEX8, int EPI, int PATH, int RULE, bool AF = false>
+__device__ __forceinline__ void fp_trace(const FpArgs& L, const kk_fp_angle* P, int a, int A, int D1, int D2, int rule,
+                                         bool a_fast, int r0, int c, int lane) {
+    float src[3], cor[3], u[3], v[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        src[k] = __ldg(&P->src[k]);
+        cor[k] = __ldg(&P->corner[k]);
+        u[k] = __ldg(&P->u[k]);
+        v[k] = __ldg(&P->v[k]);
+    }
+    const float sc1 = L.os[3 * A + 0], sc2 = L.os[3 * A + 1], oscale = L.os[3 * A + 2];
+    const int nS = L.vn[A], n1 = L.vn[D1], n2 = L.vn[D2];
+    const int64_t sS = L.vs[A], st1 = L.vs[D1], st2 = L.vs[D2];
+    const TV* vol = (const TV*)L.vol;
+    const float half1 = 0.5f * (float)n1, half2 = 0.5f * (float)n2;
+    const float unit_inv = 1.f / weight_unit<TEX8>();
+
+    // output element of ray k (row r0 + lane + 32 k)
+    auto out_ptr = [&](int k) -> TP* {
+        const int64_t off = (int64_t)(r0 + lane + 32 * k) * L.ps[1] + (int64_t)c * L.ps[2];
+        return L.table ? (TP*)L.table[a] + off : (TP*)L.out + (int64_t)a * L.ps[0] + off;
+    };
+    RaySetup R[FP_RPT];
+    float acc[FP_RPT];
+#pragma unroll
+    for (int k = 0; k < FP_RPT; ++k) {
+        const int r = r0 + lane + 32 * k;
+        const bool valid = r < L.rows;
+        R[k] = ray_setup(src, cor, u, v, A, D1, D2, valid ? r : 0, c, sc1, sc2);
+        acc[k] = (L.additive && valid) ? ld_rw(out_ptr(k)) : 0.f;
+    }
+
+    for (int off = 0; off < nS; off += L.slab) {
+        const float t1 = __fadd_rn(__fsub_rn((float)off, 0.5f * (float)nS), 0.5f);
+        const int end = min(off + L.slab, nS);
+        const float span = (float)(end - 1 - off);
+        float yc[FP_RPT], zc[FP_RPT], val[FP_RPT];
+        int cls = 2, any = 0;
+#pragma unroll
+        for (int k = 0; k < FP_RPT; ++k) {
+            yc[k] = __fadd_rn(fmaf(R[k].a1, t1, R[k].b1), half1);
+            zc[k] = __fadd_rn(fmaf(R[k].a2, t1, R[k].b2), half2);
+            val[k] = 0.f;
+            if (PATH != 0) {
+                const int cy = span_class(yc[k], fmaf(R[k].a1, span, yc[k]), n1);
+                const int cz = span_class(zc[k], fmaf(R[k].a2, span, zc[k]), n2);
+                const int ck = min(cy, cz);
+                cls = min(cls, ck);
+                any |= ck;
+            }
+        }
+        // warp-uniform choice: skip, unchecked or checked loop
+        const bool all_in = PATH != 0 && __all_sync(0xffffffffu, cls == 2);
+        const bool all_out = PATH != 0 && !__any_sync(0xffffffffu, any != 0);
+        if (all_out) continue;  // every sample is zero; the slab adds +0
+        if (PATH == 3 && FP_RPT == 2) {
+            // the texture unit filters: layer = slice, u = the faster and
+            // v = the slower in-slice axis; each fetch equals the
+            // reference's 3D-texture sample for these rays. The two rays'
+            // coordinate and sum chains advance in paired instructions.
+            float2 y2 = f2(yc[0], yc[1]), z2 = f2(zc[0], zc[1]), v2 = f2(0.f);
+            const float2 a1 = f2(R[0].a1, R[FP_RPT - 1].a1), a2 = f2(R[0].a2, R[FP_RPT - 1].a2);
+            for (int sl = off; sl < end; ++sl) {
+                const float s0 = AF ? tex2DLayered<float>(L.vtex, y2.x, z2.x, sl)
+                                    : tex2DLayered<float>(L.vtex, z2.x, y2.x, sl);
+                const float s1 = AF ? tex2DLayered<float>(L.vtex, y2.y, z2.y, sl)
+                                    : tex2DLayered<float>(L.vtex, z2.y, y2.y, sl);
+                v2 = add2(v2, f2(s0, s1));
+                y2 = add2(y2, a1);
+                z2 = add2(z2, a2);
+            }
+            val[0] = v2.x;
+            val[FP_RPT - 1] = v2.y;
+        } else if (PATH == 3) {
+            for (int sl = off; sl < end; ++sl) {
+#pragma unroll
+                for (int k = 0; k < FP_RPT; ++k) {
+                    const float uc = AF ? yc[k] : zc[k];
+                    const float vc = AF ? zc[k] : yc[k];
+                    val[k] = __fadd_rn(val[k], tex2DLayered<float>(L.vtex, uc, vc, sl));
+                    yc[k] = __fadd_rn(yc[k], R[k].a1);
+                    zc[k] = __fadd_rn(zc[k], R[k].a2);
+                }
+            }
+        } else if (PATH == 0) {
+            for (int sl = off; sl < end; ++sl) {
+                const TV* plane = vol + (int64_t)sl * sS;
+#pragma unroll
+                for (int k = 0; k < FP_RPT; ++k) {
+                    val[k] = fmaf(weight_unit<TEX8>(),
+                                  bilinear<TEX8>(plane, st1, st2, n1, n2, yc[k], zc[k], rule, a_fast), val[k]);
+                    yc[k] = __fadd_rn(yc[k], R[k].a1);
+                    zc[k] = __fadd_rn(zc[k], R[k].a2);
+                }
+            }
+        } else if (TEX8 && PATH == 2 && FP_RPT == 2 && all_in && L.off32) {
+            // Both rays of the thread share the D1 coordinate (and so its
+            // split and the two D1 rows); their D2 samples run in paired
+            // instructions. Element offsets fit 32 bits (checked on the
+            // host); the split's 0x4B4000 bias is folded into the row
+            // offset. Same operations, order and rounding as fast_sample.
+            float2 z2 = f2(zc[0], zc[1]), v2 = f2(0.f);
+            const float2 a2 = f2(R[0].a2, R[FP_RPT - 1].a2);
+            float y = yc[0];
+            const float a1 = R[0].a1;
+            const TV* vol1 = vol + st1;
+            const int st1i = (int)st1, sSi = (int)sS;
+            int soff = off * sSi - 0x4B4000;
+#pragma unroll FP_UNROLL
+            for (int sl = off; sl < end; ++sl, soff += sSi) {
+                const int yb = __float_as_int(__fadd_rd(__fmaf_rd(y, 256.f, -127.5f), 12582912.f));
+                const int rowoff = ((yb >> 8) - 0x4B4000) * st1i + soff;
+                const float S = __int_as_float((yb & 255) | 0x4B000000) - 8388608.f;
+                const float S256 = S * (1.f / 256.f);
+                const float2 m = add2_rd(fma2_rd(z2, f2(256.f), f2(-127.5f)), f2(12582912.f));
+                const int b0 = __float_as_int(m.x), b1 = __float_as_int(m.y);
+                const int o0 = (b0 >> 8) + rowoff, o1 = (b1 >> 8) + rowoff;
+                const float2 t00 = f2(ld(vol + o0), ld(vol + o1));
+                const float2 t10 = f2(ld(vol + o0 + 1), ld(vol + o1 + 1));
+                const float2 t01 = f2(ld(vol1 + o0), ld(vol1 + o1));
+                const float2 t11 = f2(ld(vol1 + o0 + 1), ld(vol1 + o1 + 1));
+                // Fr = 2^23 + F, F the fast weight (0..255)
+                const float2 Fr = f2(__int_as_float((b0 & 255) | 0x4B000000), __int_as_float((b1 & 255) | 0x4B000000));
+                const float2 F = add2(Fr, f2(-8388608.f));
+                // x1 = floor(F S / 256 + 1/2), all steps exact
+                const float2 x1 = add2(add2_rd(fma2(F, f2(S256), f2(0.5f)), f2(12582912.f)), f2(-12582912.f));
+                float2 x0;
+                if (RULE == 1)  // F + floor(1/2 - F S / 256); Fr - 2.5 * 2^23 = F - 1.5 * 2^23
+                    x0 = add2(add2_rd(fma2(F, f2(-S256), f2(0.5f)), f2(12582912.f)), add2(Fr, f2(-20971520.f)));
+                else
+                    x0 = sub2(F, x1);
+                v2 = fma2(f2(256.f), t00, v2);
+                v2 = fma2(f2(S), sub2(t01, t00), v2);
+                v2 = fma2(x1, sub2(t11, t01), v2);
+                v2 = fma2(x0, sub2(t10, t00), v2);
+                z2 = add2(z2, a2);
+                y = __fadd_rn(y, a1);
+            }
+            val[0] = v2.x;
+            val[FP_RPT - 1] = v2.y;
+        } else if (all_in) {
+#pragma unroll FP_UNROLL
+            for (int sl = off; sl < end; ++sl) {
+                const TV* plane = vol + (int64_t)sl * sS;
+                if (PATH == 2) {
+                    const Split ay = split_unclamped<TEX8>(yc[0]);
+                    const TV* row0 = plane + (int64_t)ay.i * st1;
+#pragma unroll
+                    for (int k = 0; k < FP_RPT; ++k) {
+                        val[k] = fast_sample<TEX8, false, RULE>(val[k], row0, row0 + st1, true, true, n2, ay.w, zc[k]);
+                        zc[k] = __fadd_rn(zc[k], R[k].a2);
+                    }
+                    const float ynext = __fadd_rn(yc[0], R[0].a1);
+#pragma unroll
+                    for (int k = 0; k < FP_RPT; ++k) yc[k] = ynext;
+                } else {
+#pragma unroll
+                    for (int k = 0; k < FP_RPT; ++k) {
+                        const Split ay = split_unclamped<TEX8>(yc[k]);
+                        const TV* row0 = plane + (int64_t)ay.i * st1;
+                        val[k] = fast_sample<TEX8, false, RULE>(val[k], row0, row0 + st1, true, true, n2, ay.w, zc[k]);
+                        yc[k] = __fadd_rn(yc[k], R[k].a1);
+                        zc[k] = __fadd_rn(zc[k], R[k].a2);
+                    }
+                }
+            }
+        } else {
+            for (int sl = off; sl < end; ++sl) {
+                const TV* plane = vol + (int64_t)sl * sS;
+#pragma unroll
+                for (int k = 0; k < FP_RPT; ++k) {
+                    const Split ay = split_coord<TEX8>(yc[k]);
+                    const TV* row0 = plane + (int64_t)ay.i * st1;
+                    const bool y0ok = (unsigned)ay.i < (unsigned)n1;
+                    const bool y1ok = (unsigned)(ay.i + 1) < (unsigned)n1;
+                    val[k] = fast_sample<TEX8, true, RULE>(val[k], row0, row0 + st1, y0ok, y1ok, n2, ay.w, zc[k]);
+                    yc[k] = __fadd_rn(yc[k], R[k].a1);
+                    zc[k] = __fadd_rn(zc[k], R[k].a2);
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < FP_RPT; ++k) {
+            // texture samples are plain values; the others carry weight_unit
+            const float sum = PATH == 3 ? val[k] : __fmul_rn(val[k], unit_inv);
+            acc[k] = fmaf(__fmul_rn(sum, R[k].corr), oscale, acc[k]);
+        }
+    }
+
+#pragma unroll
+    for (int k = 0; k < FP_RPT; ++k) {
+        if (r0 + lane + 32 * k >= L.rows) continue;
+        float out = acc[k];
+        if (EPI == FP_RESIDUAL) {
+            const int r = r0 + lane + 32 * k;
+            const int64_t e = (int64_t)a * L.ps[0] + (int64_t)r * L.ps[1] + (int64_t)c * L.ps[2];
+            out = __fmul_rn(__fsub_rn(out, __ldg(L.res_y + e)), __ldg(L.res_w + e));
+        }
+        st(out_ptr(k), out);
+    }
+}
+
+template <typename TV, typename TP, bool TEX8, int EPI>
+__global__ void __launch_bounds__(32 * FP_COLS, KK_FP_MINBLOCKS) cone_fp_kernel(const FpArgs L) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int t = blockIdx.x;
+    const int ct = t % L.col_tiles;
+    t /= L.col_tiles;
+    const int rec = t % L.n_angles;
+    const int rt = t / L.n_angles;
+    const int c = ct * FP_COLS + warp;
+    if (c >= L.cols) return;  // whole warp; the kernel has no block barrier
+
+    const kk_fp_angle* P = L.angles + rec;
+    const int a = __ldg(&P->index);  // projection written by this record
+    const int A = __ldg(&P->axis);
+    const int D1 = A == 1 ? 0 : 1;
+    const int D2 = A == 2 ? 0 : 2;
+    // texture weight rule of the reference's 3D texture: set by the memory
+    // rank of the slice axis (slowest: rule 0, middle: 1, fastest: 2)
+    const int rule = 2 - L.rank[A];
+    const bool a_fast = L.rank[D1] < L.rank[D2];
+    const bool fast = L.vs[D2] == 1 && rule < 2;
+    const bool shared = fast && __ldg(&P->v[A]) == 0.f && __ldg(&P->v[D1]) == 0.f;
+    const int r0 = rt * FP_ROWS_T;
+    // records flagged KK_FP_NO_TEXTURE run on the CUDA cores even when the
+    // layered texture is given, so both units share the work
+    const bool use_tex = L.vtex && L.rank[A] == 2 && !(__ldg(&P->flags) & KK_FP_NO_TEXTURE);
+    if (use_tex && a_fast)
+        fp_trace<TV, TP, TEX8, EPI, 3, 0, true>(L, P, a, A, D1, D2, rule, a_fast, r0, c, lane);
+    else if (use_tex)
+        fp_trace<TV, TP, TEX8, EPI, 3, 0, false>(L, P, a, A, D1, D2, rule, a_fast, r0, c, lane);
+    else if (shared && rule == 1)
+        fp_trace<TV, TP, TEX8, EPI, 2, 1>(L, P, a, A, D1, D2, rule, a_fast, r0, c, lane);
+    else if (shared)
+        fp_trace<TV, TP, TEX8, EPI, 2, 0>(L, P, a, A, D1, D2, rule, a_fast, r0, c, lane);
+    else if (fast && rule == 1)
+        fp_trace<TV, TP, TEX8, EPI, 1, 1>(L, P, a, A, D1, D2, rule, a_fast, r0, c, lane);
+    else if (fast)
+        fp_trace<TV, TP, TEX8, EPI, 1, 0>(L, P, a, A, D1, D2, rule, a_fast, r0, c, lane);
+    else
+        fp_trace<TV, TP, TEX8, EPI, 0, 0>(L, P, a, A, D1, D2, rule, a_fast, r0, c, lane);
+}
+
+
+}  // namespace kk
+
+// ===========================================================================
+// host side
+// ===========================================================================
+using namespace kk;
+
+template <typename TV, typename TP, int EPI>
+static void launch_fp_typed(const FpArgs& base, bool tex8, cudaStream_t s) {
+    FpArgs L = base;
+    L.col_tiles = (L.cols + FP_COLS - 1) / FP_COLS;
+    const int row_tiles = (L.rows + FP_ROWS_T - 1) / FP_ROWS_T;
+    const int64_t blocks = (int64_t)row_tiles * L.n_angles * L.col_tiles;  // < 2^31: checked by the caller
+    if (tex8)
+        cone_fp_kernel<TV, TP, true, EPI><<<(unsigned)blocks, 32 * FP_COLS, 0, s>>>(L);
+    else
+        cone_fp_kernel<TV, TP, false, EPI><<<(unsigned)blocks, 32 * FP_COLS, 0, s>>>(L);
+}
+
+template <int EPI>
+static int launch_fp(const FpArgs& L, int n_angles, int vdt, int pdt, bool tex8, cudaStream_t s) {
+#define KK_FP_CASE(VD, PD, TV, TP)                                   \
+    if (vdt == VD && pdt == PD) {                                    \
+        launch_fp_typed<TV, TP, EPI>(L, tex8, s);                    \
+        return kk_check_launch("kk_cone_fp");                         \
+    }
+    KK_FP_CASE(KK_F32, KK_F32, float, float)
+    if (EPI == FP_STORE) {
+        KK_FP_CASE(KK_BF16, KK_F32, __nv_bfloat16, float)
+        KK_FP_CASE(KK_F16, KK_F32, __half, float)
+        KK_FP_CASE(KK_BF16, KK_F16, __nv_bfloat16, __half)
+        KK_FP_CASE(KK_F16, KK_F16, __half, __half)
+        KK_FP_CASE(KK_BF16, KK_BF16, __nv_bfloat16, __nv_bfloat16)
+        KK_FP_CASE(KK_F32, KK_F16, float, __half)
+        KK_FP_CASE(KK_F32, KK_BF16, float, __nv_bfloat16)
+    }
+#undef KK_FP_CASE
+    return kk_fail(KK_ERR_UNSUPPORTED, "kk_cone_fp: dtype combination volume=%d projections=%d", vdt, pdt);
+}
+
+static int fill_fp_args(FpArgs& L, const kk_volume* vol, const kk_projections* proj, const kk_fp_angle* angles,
+                        const float* out_scale, int32_t interp, int32_t slab, const char* who) {
+    int rc = check_volume(vol, who);
+    if (rc) return rc;
+    rc = check_projections(proj, who);
+    if (rc) return rc;
+    if (!angles) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: angle parameters are NULL", who);
+    if (!out_scale) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: out_scale is NULL", who);
+    if (interp != KK_INTERP_TEX8 && interp != KK_INTERP_EXACT)
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: unknown interpolation mode %d", who, interp);
+    L = FpArgs{};
+    L.vol = vol->data;
+    for (int k = 0; k < 3; ++k) {
+        L.vs[k] = vol->stride[k];
+        L.vn[k] = (int)vol->shape[k];
+        L.ps[k] = proj->stride[k];
+    }
+    L.out = proj->data;
+    L.table = proj->table;
+    L.rows = (int)proj->rows;
+    L.cols = (int)proj->cols;
+    L.n_angles = (int)proj->n_angles;
+    L.angles = angles;
+    for (int k = 0; k < 9; ++k) L.os[k] = out_scale[k];
+    L.slab = slab > 0 ? slab : FP_SLAB;
+    if ((int64_t)((L.rows + FP_ROWS_T - 1) / FP_ROWS_T) * L.n_angles * ((L.cols + FP_COLS - 1) / FP_COLS) >=
+        0x7fffffffLL)
+        return kk_fail(KK_ERR_UNSUPPORTED, "%s: too many projection tiles for one launch", who);
+    int64_t last = 0;
+    for (int k = 0; k < 3; ++k) last += (vol->shape[k] - 1) * vol->stride[k];
+    L.off32 = last + 2 < ((int64_t)1 << 31) - 0x4B4000 && vol->stride[0] < (1 << 30) && vol->stride[1] < (1 << 30) &&
+              vol->stride[2] < (1 << 30);
+    for (int k = 0; k < 3; ++k) {
+        L.rank[k] = 0;
+        for (int j = 0; j < 3; ++j)
+            if (j != k && (vol->stride[j] < vol->stride[k] || (vol->stride[j] == vol->stride[k] && j > k)))
+                ++L.rank[k];
+    }
+    return KK_OK;
+}
+
+extern "C" int kk_cone_fp(const kk_volume* vol, const kk_projections* proj, const kk_fp_angle* angles,
+                          const float* out_scale, int32_t interp, int32_t slab, int32_t additive, void* stream) {
+    FpArgs L;
+    int rc = fill_fp_args(L, vol, proj, angles, out_scale, interp, slab, "kk_cone_fp");
+    if (rc) return rc;
+    L.additive = additive ? 1 : 0;
+    return launch_fp<FP_STORE>(L, (int)proj->n_angles, vol->dtype, proj->dtype, interp == KK_INTERP_TEX8,
+                               (cudaStream_t)stream);
+}
+
+extern "C" int kk_cone_fp_residual(const kk_volume* vol, const kk_projections* out, const kk_fp_angle* angles,
+                                   const float* out_scale, const kk_fp_residual* residual, int32_t interp,
+                                   int32_t slab, void* stream) {
+    FpArgs L;
+    int rc = fill_fp_args(L, vol, out, angles, out_scale, interp, slab, "kk_cone_fp_residual");
+    if (rc) return rc;
+    if (!residual || !residual->y || !residual->weight)
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_cone_fp_residual: residual operands are NULL");
+    if (out->table)
+        return kk_fail(KK_ERR_UNSUPPORTED, "kk_cone_fp_residual: strided projections only");
+    if (out->dtype != KK_F32 || vol->dtype != KK_F32)
+        return kk_fail(KK_ERR_UNSUPPORTED, "kk_cone_fp_residual: float32 volume and projections only");
+    L.res_y = residual->y;
+    L.res_w = residual->weight;
+    return launch_fp<FP_RESIDUAL>(L, (int)out->n_angles, vol->dtype, out->dtype, interp == KK_INTERP_TEX8,
+                                  (cudaStream_t)stream);
+}
+
+extern "C" int kk_cone_fp_layered(const kk_layered* vtex, const kk_volume* vol, const kk_projections* proj,
+                                  const kk_fp_angle* angles, const float* out_scale,
+                                  const kk_fp_residual* residual, int32_t slab, int32_t additive, void* stream) {
+    const char* who = "kk_cone_fp_layered";
+    FpArgs L;
+    int rc = fill_fp_args(L, vol, proj, angles, out_scale, KK_INTERP_TEX8, slab, who);
+    if (rc) return rc;
+    if (!vtex) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: texture is NULL", who);
+    // the texture holds the volume with one layer per slice of the slowest
+    // axis, rows along the middle axis and columns along the fastest
+    int ax_of_rank[3];
+    for (int k = 0; k < 3; ++k) ax_of_rank[L.rank[k]] = k;
+    if (vtex->layers != vol->shape[ax_of_rank[2]] || vtex->height != vol->shape[ax_of_rank[1]] ||
+        vtex->width != vol->shape[ax_of_rank[0]])
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: texture extent differs from the volume", who);
+    if ((vol->dtype == KK_F32) != (vtex->dtype == KK_F32))
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: texture and volume storage differ", who);
+    L.vtex = vtex->tex;
+    L.additive = additive ? 1 : 0;
+    if (residual) {
+        if (!residual->y || !residual->weight)
+            return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: residual operands are NULL", who);
+        if (proj->table || proj->dtype != KK_F32 || vol->dtype != KK_F32)
+            return kk_fail(KK_ERR_UNSUPPORTED, "%s: residual epilogue needs float32 strided data", who);
+        L.res_y = residual->y;
+        L.res_w = residual->weight;
+        return launch_fp<FP_RESIDUAL>(L, (int)proj->n_angles, vol->dtype, proj->dtype, true, (cudaStream_t)stream);
+    }
+    return launch_fp<FP_STORE>(L, (int)proj->n_angles, vol->dtype, proj->dtype, true, (cudaStream_t)stream);
+}
+

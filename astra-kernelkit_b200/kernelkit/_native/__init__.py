@@ -54,7 +54,9 @@ class kk_bp_update(ctypes.Structure):
 FP_ANGLE_DTYPE = np.dtype([("src", "<f4", 3), ("corner", "<f4", 3),
                            ("u", "<f4", 3), ("v", "<f4", 3),
                            ("axis", "<i4"), ("index", "<i4"),
-                           ("pad", "<i4", 2)])
+                           ("flags", "<i4"), ("pad", "<i4")])
+#: kk_fp_angle.flags bit: trace on the CUDA cores even with a texture
+KK_FP_NO_TEXTURE = 1
 #: kk_bp_angle as a NumPy record (48 bytes)
 BP_ANGLE_DTYPE = np.dtype([("num_u", "<f4", 4), ("num_v", "<f4", 4),
                            ("den", "<f4", 4)])

@@ -108,14 +108,22 @@ class RayDrivenConeFP(BaseKernel):
 
     pixels_per_block = (1, 32, 32)
     slices_per_block = 16
+    #: share of the texture-path angles traced on the CUDA cores instead,
+    #: so that the texture unit and the arithmetic pipes finish together
+    cuda_core_fraction = 0.0
 
     def __init__(self, pixels_per_block: tuple = None,
                  slices_per_block: int = None,
                  volume_axes: tuple = (0, 1, 2),
                  projection_axes: tuple = (0, 1, 2),
                  interpolation: str = "texture",
-                 use_texture_unit: bool = True):
+                 use_texture_unit: bool = True,
+                 cuda_core_fraction: float = None):
         super().__init__()
+        if cuda_core_fraction is not None:
+            if not 0.0 <= float(cuda_core_fraction) <= 1.0:
+                raise ValueError("`cuda_core_fraction` must be in [0, 1].")
+            self.cuda_core_fraction = float(cuda_core_fraction)
         # rays along the volume's slowest axis may sample a layered copy of
         # the volume through the texture unit (same filter as the
         # reference); the others run on the CUDA cores
@@ -228,11 +236,18 @@ class RayDrivenConeFP(BaseKernel):
     def _upload(self):
         """Upload the records interleaved by ray axis, so that every part
         of the launch mixes texture-unit and CUDA-core work."""
-        rec = self._host_params
+        rec = self._host_params.copy()
         key = np.empty(len(rec))
+        f = float(self.cuda_core_fraction)
         for ax in range(3):
             sel = np.flatnonzero(rec["axis"] == ax)
-            key[sel] = (np.arange(len(sel)) + 0.5) / max(len(sel), 1)
+            pos = np.arange(len(sel))
+            key[sel] = (pos + 0.5) / max(len(sel), 1)
+            # an evenly spread share of the texture-path records is traced
+            # on the CUDA cores instead (the kernel ignores the flag for
+            # records without a texture path)
+            core = np.floor((pos + 1) * f) > np.floor(pos * f)
+            rec["flags"][sel] = np.where(core, _native.KK_FP_NO_TEXTURE, 0)
         order = np.argsort(key, kind="stable")
         t = _arrays.torch()
         self._params_dev = t.from_numpy(

@@ -59,8 +59,14 @@ typedef struct {
     int32_t index;     /* projection (angle) this record writes; records
                           may come in any order, e.g. interleaved by axis
                           so every SM mixes texture and ALU work */
-    int32_t pad[2];
+    int32_t flags;     /* KK_FP_* bits below, 0 by default */
+    int32_t pad;
 } kk_fp_angle;
+
+/* kk_fp_angle.flags: trace this record on the CUDA cores even when
+ * kk_cone_fp_layered has a texture for its rays (same result), so that a
+ * caller can balance the texture unit and the arithmetic pipes. */
+#define KK_FP_NO_TEXTURE 1
 
 /* Per-angle backprojection parameters: the reference's Params struct
  * (cuda/cone_bp.cu:27-33; kernels/cone_bp.py:304-421), each float4 stored
