@@ -27,11 +27,15 @@ namespace kk {
 #ifndef KK_FP_MINBLOCKS
 #define KK_FP_MINBLOCKS 6
 #endif
+#ifndef KK_FP_TEX_UNROLL
+#define KK_FP_TEX_UNROLL 4  // slices per unrolled step of the texture loop
+#endif
 #ifndef KK_FP_UNROLL
 #define KK_FP_UNROLL 4  // slices per unrolled step of the unchecked loops
 #endif
 constexpr int FP_RPT = KK_FP_RPT;       // rays per thread
 constexpr int FP_UNROLL = KK_FP_UNROLL;
+constexpr int FP_TEX_UNROLL = KK_FP_TEX_UNROLL;
 constexpr int FP_COLS = 8;              // columns per block (one per warp)
 constexpr int FP_ROWS_T = 32 * FP_RPT;  // rows per block
 
@@ -185,6 +189,7 @@ __device__ __forceinline__ void fp_trace(const FpArgs& L, const kk_fp_angle* P, 
             // coordinate and sum chains advance in paired instructions.
             float2 y2 = f2(yc[0], yc[1]), z2 = f2(zc[0], zc[1]), v2 = f2(0.f);
             const float2 a1 = f2(R[0].a1, R[FP_RPT - 1].a1), a2 = f2(R[0].a2, R[FP_RPT - 1].a2);
+#pragma unroll FP_TEX_UNROLL
             for (int sl = off; sl < end; ++sl) {
                 const float s0 = AF ? tex2DLayered<float>(L.vtex, y2.x, z2.x, sl)
                                     : tex2DLayered<float>(L.vtex, z2.x, y2.x, sl);
