@@ -391,11 +391,15 @@ def run_ours(args):
                 "traffic": load_traffic(args.workload, "cone_fp_kernel"),
                 "algorithmic_bytes_per_launch": fp_bytes}
     kernels = {
-        "cone_fp_kernel": {"ms": t_fp, "gups": nupd / (t_fp * 1e-3) / 1e9,
+        # "traffic": ncu DRAM bytes per launch (profiles/), "ms": all
+        # launches of one operator application
+        "cone_fp_kernel": {"ms": t_fp, "launches": 1,
+                           "gups": nupd / (t_fp * 1e-3) / 1e9,
                            "achieved_gbs": fp_bytes / (t_fp * 1e-3) / 1e9,
                            "traffic": load_traffic(args.workload,
                                                    "cone_fp_kernel")},
-        "cone_bp_kernel": {"ms": t_bp, "gups": nupd / (t_bp * 1e-3) / 1e9,
+        "cone_bp_kernel": {"ms": t_bp, "launches": (len(pgs) + 31) // 32,
+                           "gups": nupd / (t_bp * 1e-3) / 1e9,
                            "achieved_gbs": fp_bytes / (t_bp * 1e-3) / 1e9,
                            "traffic": load_traffic(args.workload,
                                                    "cone_bp_kernel")},
