@@ -111,6 +111,8 @@ class RayDrivenConeFP(BaseKernel):
     #: share of the texture-path angles traced on the CUDA cores instead,
     #: so that the texture unit and the arithmetic pipes finish together
     cuda_core_fraction = 0.0
+    #: records of one ray axis launched back to back before the next axis
+    axis_group = 4
 
     def __init__(self, pixels_per_block: tuple = None,
                  slices_per_block: int = None,
@@ -239,10 +241,14 @@ class RayDrivenConeFP(BaseKernel):
         rec = self._host_params.copy()
         key = np.empty(len(rec))
         f = float(self.cuda_core_fraction)
+        g = max(int(self.axis_group), 1)
         for ax in range(3):
             sel = np.flatnonzero(rec["axis"] == ax)
             pos = np.arange(len(sel))
-            key[sel] = (pos + 0.5) / max(len(sel), 1)
+            # groups of g consecutive records of one axis alternate
+            # between the axes
+            key[sel] = ((pos // g + 0.5) / max((len(sel) + g - 1) // g, 1)
+                        + 1e-6 * ax + 1e-12 * pos)
             # an evenly spread share of the texture-path records is traced
             # on the CUDA cores instead (the kernel ignores the flag for
             # records without a texture path)
