@@ -18,7 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(os.path.dirname(HERE), "kernelkit")
 INCLUDE = os.path.join(os.path.dirname(os.path.dirname(HERE)), "include")
 OUT = os.path.join(PKG, "_native", "libkk.so")
-SOURCES = ["kk_capi.cu", "kk_fp.cu", "kk_bp.cu", "kk_fdk.cu"]
+SOURCES = ["kk_capi.cu", "kk_fp.cu", "kk_fpt.cu", "kk_bp.cu", "kk_fdk.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
                 "-Xcompiler", "-fvisibility=hidden", f"-I{INCLUDE}", f"-I{HERE}"]

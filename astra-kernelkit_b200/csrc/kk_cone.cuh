@@ -96,6 +96,35 @@ namespace kk {
 __device__ __forceinline__ float pick3(const float* v, int k) {
     return k == 0 ? v[0] : (k == 1 ? v[1] : v[2]);
 }
+
+// Ray of the forward projection through detector pixel (r, c): in-slice
+// coordinates D1 = a1 A + b1 and D2 = a2 A + b2 along the dominant axis A,
+// and the path-length correction. Shared by the projector and its exact
+// adjoint, which must see the same bits.
+struct RaySetup {
+    float a1, a2, b1, b2, corr;
+};
+
+// Per-ray slopes/offsets with the reference's float32 operation sequence
+// (cuda/cone_fp.cu:150-170, 197).
+__device__ __forceinline__ RaySetup ray_setup(const float* src, const float* cor, const float* u, const float* v,
+                                              int A, int D1, int D2, int r, int c, float sc1, float sc2) {
+    float det[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float ds = __fadd_rn(__fadd_rn(cor[k], __fmul_rn(0.5f, u[k])), __fmul_rn(0.5f, v[k]));
+        det[k] = fmaf((float)r, v[k], fmaf((float)c, u[k], ds));
+    }
+    RaySetup R;
+    const float sA = pick3(src, A), s1 = pick3(src, D1), s2 = pick3(src, D2);
+    const float sdd = __fsub_rn(sA, pick3(det, A));
+    R.a1 = __fdiv_rn(__fsub_rn(s1, pick3(det, D1)), sdd);
+    R.a2 = __fdiv_rn(__fsub_rn(s2, pick3(det, D2)), sdd);
+    R.b1 = fmaf(-R.a1, sA, s1);
+    R.b2 = fmaf(-R.a2, sA, s2);
+    R.corr = __fsqrt_rn(__fadd_rn(fmaf(__fmul_rn(R.a1, R.a1), sc1, __fmul_rn(__fmul_rn(R.a2, R.a2), sc2)), 1.f));
+    return R;
+}
 }  // namespace kk
 
 // argument checks shared by the host entry points

@@ -1,0 +1,263 @@
+// Exact adjoint of the ray-driven forward projection (kk_fp.cu), as a
+// voxel-driven gather: no atomics, every voxel sums its own terms.
+//
+// The forward projection adds, for ray (a, r, c) and every slice s along
+// the ray's dominant axis A, the bilinear sample of slice s at in-slice
+// coordinates (y_s, z_s), times corr * outputScale. Its transpose gives
+// voxel (s, j, k) the sum, over the rays whose slice-s sample touches it, of
+// proj[a, r, c] * corr * outputScale * (that sample's weight on the voxel).
+// To be the exact transpose of the forward projector (not of an idealised
+// one), each candidate ray is set up by the same ray_setup(), its slice-s
+// coordinates are rebuilt by the same slab-restart-and-increment sequence
+// in the same float32 operations, and its weights come from the same weight
+// rule (texture-compatible 1/256 weights or exact ones).
+//
+// Candidates: the footprint of voxel (j, k) in slice s is the square of
+// sample positions y in [j - 1/2, j + 3/2), z in [k - 1/2, k + 3/2); its
+// four corners are projected onto the detector and every pixel whose
+// centre falls inside their bounding box (widened by 0.05 pixel) is tested
+// exactly. Ray set-ups are computed once per chunk of angles into a
+// caller-provided work buffer, so any volume size fits by chunking.
+#include "kk_cone.cuh"
+
+namespace kk {
+
+struct FptArgs {
+    float* vol;
+    int64_t vs[3];
+    int vn[3];
+    int m0, m1, m2;  // world axes from slowest to fastest in memory
+    int rank[3];     // memory rank of each world axis: 0 fastest .. 2 slowest
+    const float* proj;
+    const uint64_t* table;
+    int64_t ps[3];
+    int rows, cols;
+    const kk_fp_angle* angles;
+    float os[9];
+    int slab;
+    int rec0, nrec;  // records of this chunk
+    int accumulate;  // add to the volume (later chunks, or additive)
+    float4* ray_ab;  // (a1, b1, a2, b2) per ray of the chunk
+    float* ray_cs;   // corr * outputScale per ray of the chunk
+};
+
+constexpr int FPT_TILE_2 = 32;
+constexpr int FPT_TILE_1 = 8;
+
+__device__ __forceinline__ void cross3(const float* a, const float* b, float* o) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+__device__ __forceinline__ float dot3(const float* a, const float* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+// Ray set-up of every (record, row, column) of the chunk.
+__global__ void fpt_rays_kernel(const FptArgs L) {
+    const int64_t per = (int64_t)L.rows * L.cols;
+    const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= per * L.nrec) return;
+    const int k = (int)(id / per);
+    const int rc = (int)(id - (int64_t)k * per);
+    const int r = rc / L.cols, c = rc - r * L.cols;
+    const kk_fp_angle* P = L.angles + L.rec0 + k;
+    float src[3], cor[3], u[3], v[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        src[q] = __ldg(&P->src[q]);
+        cor[q] = __ldg(&P->corner[q]);
+        u[q] = __ldg(&P->u[q]);
+        v[q] = __ldg(&P->v[q]);
+    }
+    const int A = __ldg(&P->axis);
+    const int D1 = A == 1 ? 0 : 1, D2 = A == 2 ? 0 : 2;
+    const RaySetup R = ray_setup(src, cor, u, v, A, D1, D2, r, c, L.os[3 * A], L.os[3 * A + 1]);
+    L.ray_ab[id] = make_float4(R.a1, R.b1, R.a2, R.b2);
+    L.ray_cs[id] = R.corr * L.os[3 * A + 2];
+}
+
+template <bool TEX8>
+__global__ void __launch_bounds__(FPT_TILE_2* FPT_TILE_1) fpt_gather_kernel(const FptArgs L) {
+    const int i2 = blockIdx.x * FPT_TILE_2 + threadIdx.x;
+    const int i1 = blockIdx.y * FPT_TILE_1 + threadIdx.y;
+    const int i0 = blockIdx.z;
+    if (i2 >= L.vn[L.m2] || i1 >= L.vn[L.m1]) return;
+    int w[3];
+    w[L.m0] = i0;
+    w[L.m1] = i1;
+    w[L.m2] = i2;
+    const int64_t per = (int64_t)L.rows * L.cols;
+    float acc = 0.f;
+    for (int k = 0; k < L.nrec; ++k) {
+        const kk_fp_angle* P = L.angles + L.rec0 + k;
+        float src[3], cor[3], u[3], v[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            src[q] = __ldg(&P->src[q]);
+            cor[q] = __ldg(&P->corner[q]);
+            u[q] = __ldg(&P->u[q]);
+            v[q] = __ldg(&P->v[q]);
+        }
+        const int A = __ldg(&P->axis);
+        const int a = __ldg(&P->index);
+        const int D1 = A == 1 ? 0 : 1, D2 = A == 2 ? 0 : 2;
+        const int s = w[A], jv = w[D1], kv = w[D2];
+        const int nS = L.vn[A], n1 = L.vn[D1], n2 = L.vn[D2];
+        const float half1 = 0.5f * (float)n1, half2 = 0.5f * (float)n2;
+        const int rule = 2 - L.rank[A];
+        const bool a_fast = L.rank[D1] < L.rank[D2];
+
+        // detector coordinates (pixel units, centre of pixel c at c + 1/2)
+        // of the footprint's corners, by central projection from the source
+        float nrm[3], e1[3], e2[3], tmp[3];
+        cross3(u, v, nrm);
+        cross3(v, nrm, tmp);
+        const float ue = dot3(u, tmp);
+        cross3(nrm, u, e2);
+        const float ve = dot3(v, e2);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            e1[q] = tmp[q] / ue;
+            e2[q] = e2[q] / ve;
+        }
+        float cs_[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) cs_[q] = cor[q] - src[q];
+        const float num = dot3(cs_, nrm);
+        const float t = (float)s - 0.5f * (float)nS + 0.5f;
+        float amin = 1e30f, amax = -1e30f, bmin = 1e30f, bmax = -1e30f;
+        bool ok = true;
+#pragma unroll
+        for (int corner = 0; corner < 4; ++corner) {
+            float p[3];
+            p[A] = t;
+            p[D1] = (float)jv - 0.5f - half1 + ((corner & 1) ? 2.f : 0.f);
+            p[D2] = (float)kv - 0.5f - half2 + ((corner & 2) ? 2.f : 0.f);
+            float d[3];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) d[q] = p[q] - src[q];
+            const float den = dot3(d, nrm);
+            const float lam = num / den;
+            ok = ok && isfinite(lam) && lam > 0.f;
+            float qc[3];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) qc[q] = src[q] + lam * d[q] - cor[q];
+            const float al = dot3(qc, e1), be = dot3(qc, e2);
+            amin = fminf(amin, al);
+            amax = fmaxf(amax, al);
+            bmin = fminf(bmin, be);
+            bmax = fmaxf(bmax, be);
+        }
+        int c0 = 0, c1 = L.cols - 1, r0 = 0, r1 = L.rows - 1;
+        if (ok && isfinite(amin) && isfinite(amax) && isfinite(bmin) && isfinite(bmax)) {
+            // pixel c is a candidate when c + 1/2 lies in [amin, amax]
+            c0 = max(c0, (int)ceilf(fmaxf(amin - 0.55f, -1.f)));
+            c1 = min(c1, (int)floorf(fminf(amax - 0.45f, (float)L.cols)));
+            r0 = max(r0, (int)ceilf(fmaxf(bmin - 0.55f, -1.f)));
+            r1 = min(r1, (int)floorf(fminf(bmax - 0.45f, (float)L.rows)));
+        }
+        const int off = (s / L.slab) * L.slab;
+        const float t1 = __fadd_rn(__fsub_rn((float)off, 0.5f * (float)nS), 0.5f);
+        const float* plane = L.table ? (const float*)L.table[a] : L.proj + (int64_t)a * L.ps[0];
+        for (int r = r0; r <= r1; ++r) {
+            for (int c = c0; c <= c1; ++c) {
+                const int64_t id = (int64_t)k * per + (int64_t)r * L.cols + c;
+                const float4 ab = __ldg(&L.ray_ab[id]);
+                // the forward projector's coordinate sequence for slice s
+                float y = __fadd_rn(fmaf(ab.x, t1, ab.y), half1);
+                float z = __fadd_rn(fmaf(ab.z, t1, ab.w), half2);
+                for (int q = off; q < s; ++q) {
+                    y = __fadd_rn(y, ab.x);
+                    z = __fadd_rn(z, ab.z);
+                }
+                const Split sy = split_coord<TEX8>(y);
+                const Split sz = split_coord<TEX8>(z);
+                const int di = jv - sy.i, dj = kv - sz.i;
+                if ((unsigned)di > 1u || (unsigned)dj > 1u) continue;
+                const W4 wt = weights4<TEX8>(sy.w, sz.w, rule, a_fast);
+                float wgt = di == 0 ? (dj == 0 ? wt.w00 : wt.w01) : (dj == 0 ? wt.w10 : wt.w11);
+                if (TEX8) wgt *= 1.f / 256.f;
+                const float p = __ldg(plane + (int64_t)r * L.ps[1] + (int64_t)c * L.ps[2]);
+                acc = fmaf(p * __ldg(&L.ray_cs[id]), wgt, acc);
+            }
+        }
+    }
+    float* out = L.vol + (int64_t)w[0] * L.vs[0] + (int64_t)w[1] * L.vs[1] + (int64_t)w[2] * L.vs[2];
+    *out = L.accumulate ? *out + acc : acc;
+}
+
+}  // namespace kk
+
+// ===========================================================================
+// host side
+// ===========================================================================
+using namespace kk;
+
+extern "C" int kk_cone_fp_adjoint(const kk_projections* proj, const kk_volume* vol, const kk_fp_angle* angles,
+                                  const float* out_scale, int32_t interp, int32_t slab, int32_t additive,
+                                  float* work, int64_t work_floats, void* stream) {
+    const char* who = "kk_cone_fp_adjoint";
+    int rc = check_volume(vol, who);
+    if (rc) return rc;
+    rc = check_projections(proj, who);
+    if (rc) return rc;
+    if (!angles || !out_scale) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: angles or out_scale is NULL", who);
+    if (interp != KK_INTERP_TEX8 && interp != KK_INTERP_EXACT)
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: unknown interpolation mode %d", who, interp);
+    if (vol->dtype != KK_F32 || proj->dtype != KK_F32)
+        return kk_fail(KK_ERR_UNSUPPORTED, "%s: float32 volume and projections only", who);
+    if (proj->table && proj->table_axis != 0)
+        return kk_fail(KK_ERR_UNSUPPORTED, "%s: pointer table along the angle axis only", who);
+    const int64_t per = proj->rows * proj->cols;
+    if (!work || ((uintptr_t)work & 15) != 0)
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: work must be a 16-byte aligned device buffer", who);
+    const int64_t chunk = work_floats / (5 * per);
+    if (chunk < 1)
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: work holds %lld floats, at least 5 * rows * cols = %lld needed",
+                       who, (long long)work_floats, (long long)(5 * per));
+    FptArgs L = {};
+    L.vol = (float*)vol->data;
+    for (int k = 0; k < 3; ++k) {
+        L.vs[k] = vol->stride[k];
+        L.vn[k] = (int)vol->shape[k];
+        L.ps[k] = proj->stride[k];
+    }
+    for (int k = 0; k < 3; ++k) {
+        L.rank[k] = 0;
+        for (int j = 0; j < 3; ++j)
+            if (j != k && (vol->stride[j] < vol->stride[k] || (vol->stride[j] == vol->stride[k] && j > k))) ++L.rank[k];
+    }
+    for (int k = 0; k < 3; ++k) {
+        if (L.rank[k] == 2) L.m0 = k;
+        if (L.rank[k] == 1) L.m1 = k;
+        if (L.rank[k] == 0) L.m2 = k;
+    }
+    if ((L.vn[L.m1] + FPT_TILE_1 - 1) / FPT_TILE_1 > MAX_GRID_Y || L.vn[L.m0] > MAX_GRID_Y)
+        return kk_fail(KK_ERR_UNSUPPORTED, "%s: volume too large for one launch", who);
+    L.proj = (const float*)proj->data;
+    L.table = proj->table;
+    L.rows = (int)proj->rows;
+    L.cols = (int)proj->cols;
+    L.angles = angles;
+    for (int k = 0; k < 9; ++k) L.os[k] = out_scale[k];
+    L.slab = slab > 0 ? slab : FP_SLAB;
+    const int n = (int)proj->n_angles;
+    const int ck = (int)std::min<int64_t>(chunk, n);
+    L.ray_ab = (float4*)work;
+    L.ray_cs = work + 4 * (int64_t)ck * per;
+    const cudaStream_t st = (cudaStream_t)stream;
+    const dim3 block(FPT_TILE_2, FPT_TILE_1);
+    const dim3 grid((L.vn[L.m2] + FPT_TILE_2 - 1) / FPT_TILE_2, (L.vn[L.m1] + FPT_TILE_1 - 1) / FPT_TILE_1, L.vn[L.m0]);
+    for (int r0 = 0; r0 < n; r0 += ck) {
+        L.rec0 = r0;
+        L.nrec = std::min(ck, n - r0);
+        L.accumulate = (r0 > 0 || additive) ? 1 : 0;
+        const int64_t rays = (int64_t)L.nrec * per;
+        fpt_rays_kernel<<<(unsigned)((rays + 255) / 256), 256, 0, st>>>(L);
+        if (interp == KK_INTERP_TEX8)
+            fpt_gather_kernel<true><<<grid, block, 0, st>>>(L);
+        else
+            fpt_gather_kernel<false><<<grid, block, 0, st>>>(L);
+    }
+    return kk_check_launch(who);
+}

@@ -63,6 +63,7 @@ BP_ANGLE_DTYPE = np.dtype([("num_u", "<f4", 4), ("num_v", "<f4", 4),
 
 #: every symbol include/kk.h declares
 EXPORTS = ("kk_cone_fp", "kk_cone_fp_residual", "kk_cone_fp_layered",
+           "kk_cone_fp_adjoint",
            "kk_cone_bp", "kk_cone_bp_static",
            "kk_cone_bp_update", "kk_layered_create", "kk_layered_copy",
            "kk_layered_destroy", "kk_cone_bp_layered",
@@ -95,6 +96,8 @@ def load():
                                       P(kk_fp_residual), i32, i32, vp]
     L.kk_cone_fp_layered.argtypes = [vp, P(kk_volume), P(kk_projections), vp,
                                      vp, P(kk_fp_residual), i32, i32, vp]
+    L.kk_cone_fp_adjoint.argtypes = [P(kk_projections), P(kk_volume), vp,
+                                     vp, i32, i32, i32, vp, i64, vp]
     L.kk_cone_bp.argtypes = [P(kk_projections), P(kk_volume), vp, f32, i32,
                              i32, vp, vp]
     L.kk_cone_bp_update.argtypes = [P(kk_projections), P(kk_volume), vp, f32,

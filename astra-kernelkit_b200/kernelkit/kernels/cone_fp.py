@@ -381,6 +381,56 @@ class RayDrivenConeFP(BaseKernel):
                 _native.current_stream()))
         del keep
 
+    #: bytes of ray set-ups the exact adjoint keeps at once (angles are
+    #: processed in chunks that fit, recomputing set-ups per chunk)
+    adjoint_work_bytes = 1 << 29
+
+    def transpose(self, projections, projection_geometry,
+                  volume_geometry: VolumeGeometry, volume,
+                  additive: bool = False):
+        """Exact adjoint of ``__call__``: ``volume = A^T projections``
+        (``+=`` with ``additive``), with exactly the weights the forward
+        projection applies, so ``<A x, y> = <x, A^T y>`` up to float32
+        rounding. ``projections`` is a float32 device array in the
+        ``projection_axes`` layout (or a list of 2D arrays), ``volume`` a
+        float32 device array in the ``volume_axes`` layout. The reference
+        has no such operator; its autograd backward is the backprojector."""
+        if not self._params_are_set:
+            raise KernelMemoryUnpreparedException(
+                "Please set the projection geometry with `set_params()`.")
+        if not isinstance(projection_geometry, ProjectionGeometrySequence):
+            projection_geometry = ProjectionGeometrySequence.fromList(
+                projection_geometry)
+        self._ensure_axes(projection_geometry, volume_geometry)
+        t = _arrays.torch()
+        vol = _arrays.as_tensor(volume)
+        vdesc = _native.volume_desc(vol, self._vol_axs)
+        expect = tuple(int(s) for s in volume_geometry.shape)
+        if tuple(vdesc.shape) != expect:
+            raise ValueError(
+                f"Volume of world shape {tuple(vdesc.shape)} does not match "
+                f"the volume geometry {expect}.")
+        pdesc, keep = self._output(projections, projection_geometry, None)
+        if pdesc.n_angles != self._n_params:
+            raise ValueError(
+                f"{pdesc.n_angles} projections given for {self._n_params} "
+                "angles.")
+        per = int(pdesc.rows) * int(pdesc.cols)
+        chunk = max(1, min(self._n_params,
+                           int(self.adjoint_work_bytes) // (20 * per)))
+        need = 5 * chunk * per
+        work = getattr(self, "_adj_work", None)
+        if work is None or work.numel() < need or work.device != vol.device:
+            work = t.empty(need, dtype=t.float32, device=vol.device)
+            self._adj_work = work
+        osc = np.asarray(self._output_scale(volume_geometry.voxel_size),
+                         np.float32).reshape(9)
+        _native.check(_native.load().kk_cone_fp_adjoint(
+            pdesc, vdesc, self._params_dev.data_ptr(), osc.ctypes.data,
+            self._interp, self.slices_per_block, int(bool(additive)),
+            work.data_ptr(), work.numel(), _native.current_stream()))
+        del keep
+
     def residual(self, volume, projection_geometry,
                  volume_geometry: VolumeGeometry, out, measured, weight):
         """Fused SIRT residual step: ``out = (A volume - measured) * weight``

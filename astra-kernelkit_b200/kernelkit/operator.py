@@ -146,5 +146,61 @@ class XrayTransform(ProjectorOperator):
         super().__init__(projector, backprojector)
 
 
+class _ExactAdjoint(BaseOperator):
+    """``A^T : Y -> X``, the exact transpose of the forward projector."""
+
+    def __init__(self, op: "ExactXrayTransform"):
+        self._op = op
+
+    @property
+    def domain_shape(self) -> tuple:
+        return self._op.range_shape
+
+    @property
+    def range_shape(self) -> tuple:
+        return self._op.domain_shape
+
+    def __call__(self, input, out=None, additive=False):
+        if tuple(input.shape) != self.domain_shape:
+            raise ValueError(
+                f"Input shape {tuple(input.shape)} does not match domain "
+                f"shape {self.domain_shape} of operator.")
+        if out is None:
+            out = _zeros(self.range_shape)
+        fp = self._op.projector
+        fp.kernel.transpose(input, fp._proj_geom_seq, fp.volume_geometry,
+                            out, additive=additive)
+        return out
+
+    @property
+    def T(self):
+        return self._op
+
+
+class ExactXrayTransform(ProjectorOperator):
+    """The cone-beam forward projection ``A`` with ``.T`` its exact
+    transpose (``RayDrivenConeFP.transpose``) instead of the reference's
+    scaled backprojector, so that ``<A x, y> = <x, A.T y>``: the operator
+    to differentiate through. Same arguments as ``XrayTransform`` (there
+    are no backprojector options)."""
+
+    def __init__(self, projection_geometry: Any, volume_geometry: Any,
+                 volume_axes: tuple = (0, 1, 2),
+                 projection_axes: tuple = (0, 1, 2), fp_kwargs=None):
+        projector = ForwardProjector(volume_axes=volume_axes,
+                                     projection_axes=projection_axes,
+                                     **dict(fp_kwargs or {}))
+        projector.volume_geometry = volume_geometry
+        projector.projection_geometry = projection_geometry
+        super().__init__(projector, None)
+
+    @property
+    def T(self):
+        if not hasattr(self, "_T"):
+            self._T = _ExactAdjoint(self)
+        return self._T
+
+
 __all__ = ["BaseOperator", "ProjectorOperator", "XrayTransform",
+           "ExactXrayTransform",
            "ForwardProjector", "BackProjector", "BaseProjector"]

@@ -3,7 +3,8 @@ reference).
 
 ``AutogradOperator`` applies an operator to every (batch, channel) slice of
 a 5D tensor; its backward applies ``op.T``, which for ``XrayTransform`` is
-the reference's (scaled, unmatched) backprojector. Everything runs on the
+the reference's (scaled, unmatched) backprojector and for
+``ExactXrayTransform`` the exact adjoint of the forward projector. Everything runs on the
 current torch stream, so the modules can be captured in CUDA graphs.
 """
 from __future__ import annotations
@@ -13,7 +14,7 @@ from itertools import product
 import torch
 from torch.autograd import Function
 
-from .operator import BaseOperator, XrayTransform
+from .operator import BaseOperator, ExactXrayTransform, XrayTransform
 
 
 class AutogradOperator(Function):
@@ -64,4 +65,22 @@ class XrayBackprojection(torch.nn.Module):
         return AutogradOperator.apply(input, self.op.T)
 
 
-__all__ = ["AutogradOperator", "XrayForwardProjection", "XrayBackprojection"]
+class ExactXrayForwardProjection(torch.nn.Module):
+    """Forward projection whose backward pass is the exact adjoint of the
+    ray-driven projector (``ExactXrayTransform``), so gradients of losses
+    on ``A x`` are the true gradients: ``<A x, y> = <x, A^T y>`` to float32
+    rounding. Arguments as ``ExactXrayTransform``. Angles are processed in
+    chunks in the backward pass, recomputing the ray set-ups per chunk, so
+    the extra memory stays bounded (``RayDrivenConeFP.adjoint_work_bytes``)
+    for any volume size."""
+
+    def __init__(self, *args, **kwargs):
+        super().__init__()
+        self.op = ExactXrayTransform(*args, **kwargs)
+
+    def forward(self, input):
+        return AutogradOperator.apply(input, self.op)
+
+
+__all__ = ["AutogradOperator", "XrayForwardProjection", "XrayBackprojection",
+           "ExactXrayForwardProjection"]

@@ -154,6 +154,21 @@ KK_API int kk_cone_fp_layered(const kk_layered* vtex, const kk_volume* vol,
                               const kk_fp_residual* residual, int32_t slab,
                               int32_t additive, void* stream);
 
+/* Exact adjoint (transpose) of kk_cone_fp for the same records,
+ * out_scale, interp and slab: vol = A^T proj (additive=0) or vol += A^T
+ * proj, bit for bit the weights kk_cone_fp applies (same ray set-up, same
+ * slab-restart coordinate sequence, same weight rule). A voxel-driven
+ * gather: every voxel sums the rays whose samples touch it, no atomics.
+ * work: 16-byte aligned float32 device scratch; the rays' set-up (5 floats
+ * per ray) is computed per chunk of angles that fits in work_floats, which
+ * must hold at least 5 * rows * cols. float32 volume and projections.
+ * The reference has no adjoint of its forward projector (its autograd
+ * backward is the unmatched backprojector, torch_support.py:29-33). */
+KK_API int kk_cone_fp_adjoint(const kk_projections* proj, const kk_volume* vol,
+                              const kk_fp_angle* angles, const float* out_scale,
+                              int32_t interp, int32_t slab, int32_t additive,
+                              float* work, int64_t work_floats, void* stream);
+
 /* ---- backprojection ------------------------------------------------- */
 
 /* Voxel-driven cone-beam backprojection (replaces VoxelDrivenConeBP.__call__,
