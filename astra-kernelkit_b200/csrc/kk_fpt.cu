@@ -38,7 +38,7 @@ struct FptArgs {
     int rec0, nrec;  // records of this chunk
     int accumulate;  // add to the volume (later chunks, or additive)
     float4* ray_ab;  // (a1, b1, a2, b2) per ray of the chunk
-    float* ray_cs;   // corr * outputScale per ray of the chunk
+    float* ray_pc;   // projection value * corr * outputScale per ray
 };
 
 constexpr int FPT_TILE_2 = 32;
@@ -52,14 +52,25 @@ __device__ __forceinline__ void cross3(const float* a, const float* b, float* o)
 
 __device__ __forceinline__ float dot3(const float* a, const float* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 
-// Ray set-up of every (record, row, column) of the chunk.
+// Component k of the point whose coordinate along axis A is t, along D1
+// is d1 and along D2 is d2 (selects, not an indexed array, so nothing goes
+// to local memory).
+__device__ __forceinline__ float place(int k, int A, int D1, float t, float d1, float d2) {
+    return k == A ? t : (k == D1 ? d1 : d2);
+}
+
+// Ray set-up of every (record, column, row) of the chunk, rows fastest: a
+// warp of the gather (consecutive voxels along the fastest volume axis,
+// which for circular scans map to consecutive detector rows) then reads
+// neighbouring entries. The projection value is folded in here, times the
+// ray's corr * outputScale.
 __global__ void fpt_rays_kernel(const FptArgs L) {
     const int64_t per = (int64_t)L.rows * L.cols;
     const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= per * L.nrec) return;
     const int k = (int)(id / per);
-    const int rc = (int)(id - (int64_t)k * per);
-    const int r = rc / L.cols, c = rc - r * L.cols;
+    const int cr = (int)(id - (int64_t)k * per);
+    const int c = cr / L.rows, r = cr - c * L.rows;
     const kk_fp_angle* P = L.angles + L.rec0 + k;
     float src[3], cor[3], u[3], v[3];
 #pragma unroll
@@ -72,8 +83,11 @@ __global__ void fpt_rays_kernel(const FptArgs L) {
     const int A = __ldg(&P->axis);
     const int D1 = A == 1 ? 0 : 1, D2 = A == 2 ? 0 : 2;
     const RaySetup R = ray_setup(src, cor, u, v, A, D1, D2, r, c, L.os[3 * A], L.os[3 * A + 1]);
+    const int a = __ldg(&P->index);
+    const float* plane = L.table ? (const float*)L.table[a] : L.proj + (int64_t)a * L.ps[0];
+    const float p = __ldg(plane + (int64_t)r * L.ps[1] + (int64_t)c * L.ps[2]);
     L.ray_ab[id] = make_float4(R.a1, R.b1, R.a2, R.b2);
-    L.ray_cs[id] = R.corr * L.os[3 * A + 2];
+    L.ray_pc[id] = p * (R.corr * L.os[3 * A + 2]);
 }
 
 template <bool TEX8>
@@ -82,10 +96,10 @@ __global__ void __launch_bounds__(FPT_TILE_2* FPT_TILE_1) fpt_gather_kernel(cons
     const int i1 = blockIdx.y * FPT_TILE_1 + threadIdx.y;
     const int i0 = blockIdx.z;
     if (i2 >= L.vn[L.m2] || i1 >= L.vn[L.m1]) return;
-    int w[3];
-    w[L.m0] = i0;
-    w[L.m1] = i1;
-    w[L.m2] = i2;
+    // world indices of the voxel
+    const int w0 = L.m0 == 0 ? i0 : (L.m1 == 0 ? i1 : i2);
+    const int w1 = L.m0 == 1 ? i0 : (L.m1 == 1 ? i1 : i2);
+    const int w2 = L.m0 == 2 ? i0 : (L.m1 == 2 ? i1 : i2);
     const int64_t per = (int64_t)L.rows * L.cols;
     float acc = 0.f;
     for (int k = 0; k < L.nrec; ++k) {
@@ -99,13 +113,19 @@ __global__ void __launch_bounds__(FPT_TILE_2* FPT_TILE_1) fpt_gather_kernel(cons
             v[q] = __ldg(&P->v[q]);
         }
         const int A = __ldg(&P->axis);
-        const int a = __ldg(&P->index);
         const int D1 = A == 1 ? 0 : 1, D2 = A == 2 ? 0 : 2;
-        const int s = w[A], jv = w[D1], kv = w[D2];
-        const int nS = L.vn[A], n1 = L.vn[D1], n2 = L.vn[D2];
+        const int s = A == 0 ? w0 : (A == 1 ? w1 : w2);
+        const int jv = D1 == 0 ? w0 : w1;
+        const int kv = D2 == 0 ? w0 : w2;
+        const int nS = A == 0 ? L.vn[0] : (A == 1 ? L.vn[1] : L.vn[2]);
+        const int n1 = D1 == 0 ? L.vn[0] : L.vn[1];
+        const int n2 = D2 == 0 ? L.vn[0] : L.vn[2];
         const float half1 = 0.5f * (float)n1, half2 = 0.5f * (float)n2;
-        const int rule = 2 - L.rank[A];
-        const bool a_fast = L.rank[D1] < L.rank[D2];
+        const int rA = A == 0 ? L.rank[0] : (A == 1 ? L.rank[1] : L.rank[2]);
+        const int r1 = D1 == 0 ? L.rank[0] : L.rank[1];
+        const int r2 = D2 == 0 ? L.rank[0] : L.rank[2];
+        const int rule = 2 - rA;
+        const bool a_fast = r1 < r2;
 
         // detector coordinates (pixel units, centre of pixel c at c + 1/2)
         // of the footprint's corners, by central projection from the source
@@ -115,10 +135,13 @@ __global__ void __launch_bounds__(FPT_TILE_2* FPT_TILE_1) fpt_gather_kernel(cons
         const float ue = dot3(u, tmp);
         cross3(nrm, u, e2);
         const float ve = dot3(v, e2);
+        // the candidate box only needs a few correct digits (it is widened
+        // by 0.05 pixel), so the fast reciprocal and division suffice
+        const float iue = __frcp_rn(ue), ive = __frcp_rn(ve);
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
-            e1[q] = tmp[q] / ue;
-            e2[q] = e2[q] / ve;
+            e1[q] = tmp[q] * iue;
+            e2[q] = e2[q] * ive;
         }
         float cs_[3];
 #pragma unroll
@@ -129,15 +152,13 @@ __global__ void __launch_bounds__(FPT_TILE_2* FPT_TILE_1) fpt_gather_kernel(cons
         bool ok = true;
 #pragma unroll
         for (int corner = 0; corner < 4; ++corner) {
-            float p[3];
-            p[A] = t;
-            p[D1] = (float)jv - 0.5f - half1 + ((corner & 1) ? 2.f : 0.f);
-            p[D2] = (float)kv - 0.5f - half2 + ((corner & 2) ? 2.f : 0.f);
+            const float d1 = (float)jv - 0.5f - half1 + ((corner & 1) ? 2.f : 0.f);
+            const float d2 = (float)kv - 0.5f - half2 + ((corner & 2) ? 2.f : 0.f);
             float d[3];
 #pragma unroll
-            for (int q = 0; q < 3; ++q) d[q] = p[q] - src[q];
+            for (int q = 0; q < 3; ++q) d[q] = place(q, A, D1, t, d1, d2) - src[q];
             const float den = dot3(d, nrm);
-            const float lam = num / den;
+            const float lam = __fdividef(num, den);
             ok = ok && isfinite(lam) && lam > 0.f;
             float qc[3];
 #pragma unroll
@@ -148,27 +169,68 @@ __global__ void __launch_bounds__(FPT_TILE_2* FPT_TILE_1) fpt_gather_kernel(cons
             bmin = fminf(bmin, be);
             bmax = fmaxf(bmax, be);
         }
-        int c0 = 0, c1 = L.cols - 1, r0 = 0, r1 = L.rows - 1;
+        int c0 = 0, c1 = L.cols - 1, rlo = 0, rhi = L.rows - 1;
         if (ok && isfinite(amin) && isfinite(amax) && isfinite(bmin) && isfinite(bmax)) {
             // pixel c is a candidate when c + 1/2 lies in [amin, amax]
             c0 = max(c0, (int)ceilf(fmaxf(amin - 0.55f, -1.f)));
             c1 = min(c1, (int)floorf(fminf(amax - 0.45f, (float)L.cols)));
-            r0 = max(r0, (int)ceilf(fmaxf(bmin - 0.55f, -1.f)));
-            r1 = min(r1, (int)floorf(fminf(bmax - 0.45f, (float)L.rows)));
+            rlo = max(rlo, (int)ceilf(fmaxf(bmin - 0.55f, -1.f)));
+            rhi = min(rhi, (int)floorf(fminf(bmax - 0.45f, (float)L.rows)));
         }
         const int off = (s / L.slab) * L.slab;
         const float t1 = __fadd_rn(__fsub_rn((float)off, 0.5f * (float)nS), 0.5f);
-        const float* plane = L.table ? (const float*)L.table[a] : L.proj + (int64_t)a * L.ps[0];
-        for (int r = r0; r <= r1; ++r) {
-            for (int c = c0; c <= c1; ++c) {
-                const int64_t id = (int64_t)k * per + (int64_t)r * L.cols + c;
+        // circular scans: the detector's v has no component along A and D1,
+        // so every row of a column has bit for bit the same D1 coordinate
+        // sequence (as in the forward projector's shared path); a column
+        // whose D1 sample misses the voxel is then skipped whole
+        const float vA = A == 0 ? v[0] : (A == 1 ? v[1] : v[2]);
+        const float vD1 = D1 == 0 ? v[0] : v[1];
+        const bool shared = vA == 0.f && vD1 == 0.f;
+        for (int c = c0; c <= c1; ++c) {
+            if (shared && rlo <= rhi) {
+                const float4 ab = __ldg(&L.ray_ab[(int64_t)k * per + (int64_t)c * L.rows + rlo]);
+                float y = __fadd_rn(fmaf(ab.x, t1, ab.y), half1);
+                for (int q = off; q < s; ++q) y = __fadd_rn(y, ab.x);
+                const int di = jv - split_coord<TEX8>(y).i;
+                if ((unsigned)di > 1u) continue;
+            }
+            for (int r = rlo; r <= rhi; ++r) {
+                const int64_t id = (int64_t)k * per + (int64_t)c * L.rows + r;
                 const float4 ab = __ldg(&L.ray_ab[id]);
-                // the forward projector's coordinate sequence for slice s
+                // the forward projector's coordinate sequence for slice s:
+                // the slab-start value, then one rounded add per slice
                 float y = __fadd_rn(fmaf(ab.x, t1, ab.y), half1);
                 float z = __fadd_rn(fmaf(ab.z, t1, ab.w), half2);
-                for (int q = off; q < s; ++q) {
-                    y = __fadd_rn(y, ab.x);
-                    z = __fadd_rn(z, ab.z);
+                bool chain = true;
+                if (TEX8) {
+                    // The texture-compatible split only sees
+                    // floor(256 y - 127.5). Each of the nst rounded adds
+                    // errs by at most half an ulp (2^-24 relative), so the
+                    // chain ends within eps of fma(nst, a, y0); when no
+                    // boundary of floor() lies within that distance, the
+                    // direct value splits exactly as the chain would.
+                    const float nst = (float)(s - off);
+                    const float yd = fmaf(nst, ab.x, y), zd = fmaf(nst, ab.z, z);
+                    const float eps = (nst + 1.f) * 1.2e-7f * (fmaxf(fabsf(yd), fabsf(zd)) + fabsf(ab.x) * nst +
+                                                                  fabsf(ab.z) * nst + 1.f);
+                    // for |y| < 2^13, q = 256 y - 127.5 and q - floor(q)
+                    // are exact in float32, so the distance to the next
+                    // boundary is known exactly
+                    const float qy = 256.f * yd - 127.5f, qz = 256.f * zd - 127.5f;
+                    const float fy = qy - floorf(qy), fz = qz - floorf(qz);
+                    const float e = 256.f * 1.01f * eps + 1e-6f;
+                    if (fabsf(yd) < 8192.f && fabsf(zd) < 8192.f && fy > e && fy < 1.f - e && fz > e &&
+                        fz < 1.f - e) {
+                        y = yd;
+                        z = zd;
+                        chain = false;
+                    }
+                }
+                if (chain) {
+                    for (int q = off; q < s; ++q) {
+                        y = __fadd_rn(y, ab.x);
+                        z = __fadd_rn(z, ab.z);
+                    }
                 }
                 const Split sy = split_coord<TEX8>(y);
                 const Split sz = split_coord<TEX8>(z);
@@ -177,12 +239,11 @@ __global__ void __launch_bounds__(FPT_TILE_2* FPT_TILE_1) fpt_gather_kernel(cons
                 const W4 wt = weights4<TEX8>(sy.w, sz.w, rule, a_fast);
                 float wgt = di == 0 ? (dj == 0 ? wt.w00 : wt.w01) : (dj == 0 ? wt.w10 : wt.w11);
                 if (TEX8) wgt *= 1.f / 256.f;
-                const float p = __ldg(plane + (int64_t)r * L.ps[1] + (int64_t)c * L.ps[2]);
-                acc = fmaf(p * __ldg(&L.ray_cs[id]), wgt, acc);
+                acc = fmaf(__ldg(&L.ray_pc[id]), wgt, acc);
             }
         }
     }
-    float* out = L.vol + (int64_t)w[0] * L.vs[0] + (int64_t)w[1] * L.vs[1] + (int64_t)w[2] * L.vs[2];
+    float* out = L.vol + (int64_t)w0 * L.vs[0] + (int64_t)w1 * L.vs[1] + (int64_t)w2 * L.vs[2];
     *out = L.accumulate ? *out + acc : acc;
 }
 
@@ -244,7 +305,7 @@ extern "C" int kk_cone_fp_adjoint(const kk_projections* proj, const kk_volume* v
     const int n = (int)proj->n_angles;
     const int ck = (int)std::min<int64_t>(chunk, n);
     L.ray_ab = (float4*)work;
-    L.ray_cs = work + 4 * (int64_t)ck * per;
+    L.ray_pc = work + 4 * (int64_t)ck * per;
     const cudaStream_t st = (cudaStream_t)stream;
     const dim3 block(FPT_TILE_2, FPT_TILE_1);
     const dim3 grid((L.vn[L.m2] + FPT_TILE_2 - 1) / FPT_TILE_2, (L.vn[L.m1] + FPT_TILE_1 - 1) / FPT_TILE_1, L.vn[L.m0]);
