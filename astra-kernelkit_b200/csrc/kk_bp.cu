@@ -11,16 +11,16 @@ namespace kk {
 // BP_GROUP voxels along the slowest memory axis
 // ---------------------------------------------------------------------------
 template <typename TP, typename TV, bool TEX8, int EPI, int FETCH>
-__global__ void __launch_bounds__(BP_TILE_2* BP_TILE_1) cone_bp_kernel(const BpArgs L) {
+__device__ __forceinline__ void bp_block(const BpArgs& L, int bx, int by, int bz) {
     // One launch covers the angles [j_begin, j_end): one 32-angle chunk,
     // as one launch of the reference does (kernels/cone_bp.py:297-302), so
     // the chunk's projections stay in L2 while every voxel reads them; the
     // running sum vol += acc * scale is carried between launches in the
     // volume (float32) or in the float32 work buffer.
     __shared__ kk_bp_angle sp[BP_CHUNK];
-    const int i2 = blockIdx.x * BP_TILE_2 + threadIdx.x;
-    const int i1 = blockIdx.y * BP_TILE_1 + threadIdx.y;
-    const int g0 = blockIdx.z * BP_GROUP;
+    const int i2 = bx * BP_TILE_2 + threadIdx.x;
+    const int i1 = by * BP_TILE_1 + threadIdx.y;
+    const int g0 = bz * BP_GROUP;
     const int n0 = L.vn[L.m0], n1 = L.vn[L.m1], n2 = L.vn[L.m2];
     const bool active = i2 < n2 && i1 < n1;
     const int cnt = min(BP_GROUP, n0 - g0);
@@ -113,6 +113,37 @@ __global__ void __launch_bounds__(BP_TILE_2* BP_TILE_1) cone_bp_kernel(const BpA
             st(p, vacc[i]);
         }
     }
+}
+
+template <typename TP, typename TV, bool TEX8, int EPI, int FETCH>
+__global__ void __launch_bounds__(BP_TILE_2* BP_TILE_1) cone_bp_kernel(const BpArgs L) {
+    bp_block<TP, TV, TEX8, EPI, FETCH>(L, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// Many problems in one launch (one 32-angle chunk of each): argument
+// blocks in the kernel's parameter space, as for the batched forward
+// projection; tiles[i] = (x tiles, y tiles) of problem i's grid.
+struct BpBatch {
+    int n;
+    int block_start[KK_MAX_BATCH + 1];
+    int tiles[KK_MAX_BATCH][2];
+    BpArgs p[KK_MAX_BATCH];
+};
+
+template <int EPI>
+__global__ void __launch_bounds__(BP_TILE_2* BP_TILE_1) cone_bp_batched_kernel(const __grid_constant__ BpBatch B) {
+    __shared__ BpArgs Ls;
+    const int b = blockIdx.x;
+    int i = 0;
+    while (i + 1 < B.n && B.block_start[i + 1] <= b) ++i;
+    static_assert(sizeof(BpArgs) % 4 == 0 && sizeof(BpArgs) <= 4 * BP_TILE_2 * BP_TILE_1, "argument copy");
+    const int tid = threadIdx.y * BP_TILE_2 + threadIdx.x;
+    const int* src = reinterpret_cast<const int*>(&B.p[i]);
+    for (int k = tid; k < (int)(sizeof(BpArgs) / 4); k += BP_TILE_2 * BP_TILE_1) reinterpret_cast<int*>(&Ls)[k] = src[k];
+    __syncthreads();
+    const int t = b - B.block_start[i];
+    const int tx = B.tiles[i][0], ty = B.tiles[i][1];
+    bp_block<float, float, true, EPI, FETCH_TEX>(Ls, t % tx, (t / tx) % ty, t / (tx * ty));
 }
 
 }  // namespace kk
@@ -447,4 +478,71 @@ extern "C" int kk_cone_bp_static(const kk_projections* proj, const kk_volume* vo
     // same call wrote, and the first chunk starts from zero or the volume,
     // so the buffer's previous contents never matter
     return kk_cone_bp(proj, vol, angles, out_scale, interp, additive, scratch, stream);
+}
+
+extern "C" int kk_cone_bp_layered_batched(const kk_bp_problem* pr, int32_t n, void* stream) {
+    const char* who = "kk_cone_bp_layered_batched";
+    if (!pr || n < 1 || n > KK_MAX_BATCH)
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: need 1..%d problems, got %d", who, KK_MAX_BATCH, n);
+    BpArgs args[KK_MAX_BATCH];
+    int chunks[KK_MAX_BATCH];
+    int max_chunks = 0;
+    for (int i = 0; i < n; ++i) {
+        const kk_bp_problem& q = pr[i];
+        if (q.vol.dtype != KK_F32) return kk_fail(KK_ERR_UNSUPPORTED, "%s: problem %d: float32 volume only", who, i);
+        int rc = layered_args(args[i], q.tex, &q.vol, q.angles, q.out_scale, who);
+        if (rc) return rc;
+        BpArgs& L = args[i];
+        const bool update = q.update.scale != nullptr;
+        L.upd_scale = q.update.scale;
+        L.upd_mask = q.update.mask;
+        L.vmin = q.update.min_value;
+        L.vmax = q.update.max_value;
+        L.has_min = q.update.has_min;
+        L.has_max = q.update.has_max;
+        L.work = q.work;
+        chunks[i] = (L.n_angles + BP_CHUNK - 1) / BP_CHUNK;
+        if (update && chunks[i] > 1 && !q.work)
+            return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: problem %d: an update over %d angles needs work", who, i,
+                           L.n_angles);
+        max_chunks = max(max_chunks, chunks[i]);
+    }
+    const cudaStream_t st = (cudaStream_t)stream;
+    for (int c = 0; c < max_chunks; ++c) {
+        for (int kind = 0; kind < 2; ++kind) {  // plain, then update problems
+            BpBatch B;
+            B.n = 0;
+            int64_t total = 0;
+            for (int i = 0; i < n; ++i) {
+                const bool update = pr[i].update.scale != nullptr;
+                if (update != (kind == 1) || c >= chunks[i]) continue;
+                BpArgs L = args[i];
+                // as bp_chunks() for a float32 volume
+                const bool need_work = chunks[i] > 1 && update;
+                const int first_load = (pr[i].additive && !update) ? LOAD_VOL : LOAD_ZERO;
+                L.j_begin = c * BP_CHUNK;
+                L.j_end = min(L.n_angles, L.j_begin + BP_CHUNK);
+                L.load_mode = c == 0 ? first_load : (need_work ? LOAD_WORK : LOAD_VOL);
+                L.store_mode = c == chunks[i] - 1 ? STORE_FINAL : (need_work ? STORE_WORK : STORE_VOL);
+                const dim3 g = bp_grid(L);
+                B.p[B.n] = L;
+                B.tiles[B.n][0] = (int)g.x;
+                B.tiles[B.n][1] = (int)g.y;
+                B.block_start[B.n] = (int)total;
+                total += (int64_t)g.x * g.y * g.z;
+                ++B.n;
+                if (total >= 0x7fffffffLL) return kk_fail(KK_ERR_UNSUPPORTED, "%s: too many blocks for one launch", who);
+            }
+            if (B.n == 0) continue;
+            B.block_start[B.n] = (int)total;
+            const dim3 block(BP_TILE_2, BP_TILE_1);
+            if (kind == 0)
+                cone_bp_batched_kernel<BP_STORE><<<(unsigned)total, block, 0, st>>>(B);
+            else
+                cone_bp_batched_kernel<BP_UPDATE><<<(unsigned)total, block, 0, st>>>(B);
+            const int rc = kk_check_launch(who);
+            if (rc) return rc;
+        }
+    }
+    return KK_OK;
 }

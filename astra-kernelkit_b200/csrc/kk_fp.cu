@@ -306,9 +306,8 @@ __device__ __forceinline__ void fp_trace(const FpArgs& L, const kk_fp_angle* P, 
 }
 
 template <typename TV, typename TP, bool TEX8, int EPI>
-__global__ void __launch_bounds__(32 * FP_COLS, KK_FP_MINBLOCKS) cone_fp_kernel(const FpArgs L) {
+__device__ __forceinline__ void fp_block(const FpArgs& L, int t) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int t = blockIdx.x;
     const int ct = t % L.col_tiles;
     t /= L.col_tiles;
     const int rec = t % L.n_angles;
@@ -345,6 +344,34 @@ __global__ void __launch_bounds__(32 * FP_COLS, KK_FP_MINBLOCKS) cone_fp_kernel(
         fp_trace<TV, TP, TEX8, EPI, 1, 0>(L, P, a, A, D1, D2, rule, a_fast, r0, c, lane);
     else
         fp_trace<TV, TP, TEX8, EPI, 0, 0>(L, P, a, A, D1, D2, rule, a_fast, r0, c, lane);
+}
+
+template <typename TV, typename TP, bool TEX8, int EPI>
+__global__ void __launch_bounds__(32 * FP_COLS, KK_FP_MINBLOCKS) cone_fp_kernel(const FpArgs L) {
+    fp_block<TV, TP, TEX8, EPI>(L, blockIdx.x);
+}
+
+// Many problems in one launch: the argument blocks of up to KK_MAX_BATCH
+// projections travel in the kernel's parameter space (no device memory),
+// each block finds its problem from the prefix block counts and copies that
+// problem's arguments to shared memory before tracing.
+struct FpBatch {
+    int n;
+    int block_start[KK_MAX_BATCH + 1];
+    FpArgs p[KK_MAX_BATCH];
+};
+
+template <bool TEX8, int EPI>
+__global__ void __launch_bounds__(32 * FP_COLS, 4) cone_fp_batched_kernel(const __grid_constant__ FpBatch B) {
+    __shared__ FpArgs Ls;
+    const int b = blockIdx.x;
+    int i = 0;
+    while (i + 1 < B.n && B.block_start[i + 1] <= b) ++i;
+    static_assert(sizeof(FpArgs) % 4 == 0 && sizeof(FpArgs) <= 4 * 32 * FP_COLS, "argument copy");
+    const int* src = reinterpret_cast<const int*>(&B.p[i]);
+    for (int k = threadIdx.x; k < (int)(sizeof(FpArgs) / 4); k += blockDim.x) reinterpret_cast<int*>(&Ls)[k] = src[k];
+    __syncthreads();
+    fp_block<float, float, TEX8, EPI>(Ls, b - B.block_start[i]);
 }
 
 
@@ -488,3 +515,64 @@ extern "C" int kk_cone_fp_layered(const kk_layered* vtex, const kk_volume* vol, 
     return launch_fp<FP_STORE>(L, (int)proj->n_angles, vol->dtype, proj->dtype, true, (cudaStream_t)stream);
 }
 
+extern "C" int kk_cone_fp_batched(const kk_fp_problem* pr, int32_t n, int32_t interp, int32_t slab, void* stream) {
+    const char* who = "kk_cone_fp_batched";
+    if (!pr || n < 1 || n > KK_MAX_BATCH)
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: need 1..%d problems, got %d", who, KK_MAX_BATCH, n);
+    const cudaStream_t st = (cudaStream_t)stream;
+    for (int kind = 0; kind < 2; ++kind) {  // plain, then residual problems
+        FpBatch B;  // about 14 KB, copied into the launch's parameters
+        B.n = 0;
+        int64_t total = 0;
+        for (int i = 0; i < n; ++i) {
+            const kk_fp_problem& q = pr[i];
+            const bool res = q.residual.y || q.residual.weight;
+            if (res != (kind == 1)) continue;
+            FpArgs L;
+            int rc = fill_fp_args(L, &q.vol, &q.proj, q.angles, q.out_scale, interp, slab, who);
+            if (rc) return rc;
+            if (q.vol.dtype != KK_F32 || q.proj.dtype != KK_F32)
+                return kk_fail(KK_ERR_UNSUPPORTED, "%s: problem %d: float32 volume and projections only", who, i);
+            if (q.vtex) {
+                int ax_of_rank[3];
+                for (int k = 0; k < 3; ++k) ax_of_rank[L.rank[k]] = k;
+                if (interp != KK_INTERP_TEX8 || q.vtex->dtype != KK_F32 || q.vtex->layers != q.vol.shape[ax_of_rank[2]] ||
+                    q.vtex->height != q.vol.shape[ax_of_rank[1]] || q.vtex->width != q.vol.shape[ax_of_rank[0]])
+                    return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: problem %d: texture does not match the volume", who, i);
+                L.vtex = q.vtex->tex;
+            }
+            if (res) {
+                if (!q.residual.y || !q.residual.weight || q.proj.table)
+                    return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: problem %d: residual needs y, weight, strided data",
+                                   who, i);
+                L.res_y = q.residual.y;
+                L.res_w = q.residual.weight;
+            }
+            L.additive = q.additive ? 1 : 0;
+            L.col_tiles = (L.cols + FP_COLS - 1) / FP_COLS;
+            const int64_t blocks = (int64_t)((L.rows + FP_ROWS_T - 1) / FP_ROWS_T) * L.n_angles * L.col_tiles;
+            B.p[B.n] = L;
+            B.block_start[B.n] = (int)total;
+            total += blocks;
+            ++B.n;
+            if (total >= 0x7fffffffLL) return kk_fail(KK_ERR_UNSUPPORTED, "%s: too many blocks for one launch", who);
+        }
+        if (B.n == 0) continue;
+        B.block_start[B.n] = (int)total;
+        const bool tex8 = interp == KK_INTERP_TEX8;
+        if (kind == 0) {
+            if (tex8)
+                cone_fp_batched_kernel<true, FP_STORE><<<(unsigned)total, 32 * FP_COLS, 0, st>>>(B);
+            else
+                cone_fp_batched_kernel<false, FP_STORE><<<(unsigned)total, 32 * FP_COLS, 0, st>>>(B);
+        } else {
+            if (tex8)
+                cone_fp_batched_kernel<true, FP_RESIDUAL><<<(unsigned)total, 32 * FP_COLS, 0, st>>>(B);
+            else
+                cone_fp_batched_kernel<false, FP_RESIDUAL><<<(unsigned)total, 32 * FP_COLS, 0, st>>>(B);
+        }
+        const int rc = kk_check_launch(who);
+        if (rc) return rc;
+    }
+    return KK_OK;
+}

@@ -50,6 +50,24 @@ class kk_bp_update(ctypes.Structure):
                 ("has_min", ctypes.c_int32), ("has_max", ctypes.c_int32)]
 
 
+#: most problems one batched call takes (KK_MAX_BATCH of include/kk.h)
+KK_MAX_BATCH = 64
+
+
+class kk_fp_problem(ctypes.Structure):
+    _fields_ = [("vol", kk_volume), ("proj", kk_projections),
+                ("angles", ctypes.c_void_p),
+                ("out_scale", ctypes.c_float * 9), ("vtex", ctypes.c_void_p),
+                ("residual", kk_fp_residual), ("additive", ctypes.c_int32)]
+
+
+class kk_bp_problem(ctypes.Structure):
+    _fields_ = [("tex", ctypes.c_void_p), ("vol", kk_volume),
+                ("angles", ctypes.c_void_p), ("out_scale", ctypes.c_float),
+                ("update", kk_bp_update), ("work", ctypes.c_void_p),
+                ("additive", ctypes.c_int32)]
+
+
 #: kk_fp_angle as a NumPy record (64 bytes)
 FP_ANGLE_DTYPE = np.dtype([("src", "<f4", 3), ("corner", "<f4", 3),
                            ("u", "<f4", 3), ("v", "<f4", 3),
@@ -63,7 +81,8 @@ BP_ANGLE_DTYPE = np.dtype([("num_u", "<f4", 4), ("num_v", "<f4", 4),
 
 #: every symbol include/kk.h declares
 EXPORTS = ("kk_cone_fp", "kk_cone_fp_residual", "kk_cone_fp_layered",
-           "kk_cone_fp_adjoint",
+           "kk_cone_fp_adjoint", "kk_cone_fp_batched",
+           "kk_cone_bp_layered_batched",
            "kk_cone_bp", "kk_cone_bp_static",
            "kk_cone_bp_update", "kk_layered_create", "kk_layered_copy",
            "kk_layered_destroy", "kk_cone_bp_layered",
@@ -98,6 +117,8 @@ def load():
                                      vp, P(kk_fp_residual), i32, i32, vp]
     L.kk_cone_fp_adjoint.argtypes = [P(kk_projections), P(kk_volume), vp,
                                      vp, i32, i32, i32, vp, i64, vp]
+    L.kk_cone_fp_batched.argtypes = [P(kk_fp_problem), i32, i32, i32, vp]
+    L.kk_cone_bp_layered_batched.argtypes = [P(kk_bp_problem), i32, vp]
     L.kk_cone_bp.argtypes = [P(kk_projections), P(kk_volume), vp, f32, i32,
                              i32, vp, vp]
     L.kk_cone_bp_update.argtypes = [P(kk_projections), P(kk_volume), vp, f32,

@@ -233,6 +233,51 @@ KK_API int kk_cone_bp_layered_update(const kk_layered* tex,
                                      const kk_bp_update* update, float* work,
                                      void* stream);
 
+/* ---- batches of independent problems ------------------------------------ */
+
+/* Many volumes and scans of different sizes in one launch: the argument
+ * blocks of up to KK_MAX_BATCH problems travel in the kernel parameters
+ * (nothing is allocated), and each thread block finds its own problem.
+ * The reference runs one problem per call; it has no counterpart. */
+#define KK_MAX_BATCH 64
+
+typedef struct {
+    kk_volume vol;              /* float32 */
+    kk_projections proj;        /* float32 output */
+    const kk_fp_angle* angles;  /* this problem's records (device) */
+    float out_scale[9];         /* as kk_cone_fp */
+    const kk_layered* vtex;     /* layered copy of the volume for rays along
+                                   its slowest axis (as kk_cone_fp_layered),
+                                   or NULL */
+    kk_fp_residual residual;    /* y and weight NULL: plain projection */
+    int32_t additive;
+} kk_fp_problem;
+
+/* kk_cone_fp / kk_cone_fp_layered / kk_cone_fp_residual for n problems
+ * (1 <= n <= KK_MAX_BATCH) in at most two launches (plain and residual
+ * problems are launched apart). Results equal the one-problem calls. */
+KK_API int kk_cone_fp_batched(const kk_fp_problem* problems, int32_t n,
+                              int32_t interp, int32_t slab, void* stream);
+
+typedef struct {
+    const kk_layered* tex;      /* the projections (kk_layered_copy) */
+    kk_volume vol;              /* float32 */
+    const kk_bp_angle* angles;
+    float out_scale;            /* as kk_cone_bp */
+    kk_bp_update update;        /* update.scale NULL: plain backprojection */
+    float* work;                /* float32 running sums, one per voxel;
+                                   required for an update over more than
+                                   32 angles */
+    int32_t additive;
+} kk_bp_problem;
+
+/* kk_cone_bp_layered / kk_cone_bp_layered_update for n problems: one
+ * launch per 32-angle chunk index, covering that chunk of every problem
+ * that has it (plain and update problems launched apart). Results equal
+ * the one-problem calls. */
+KK_API int kk_cone_bp_layered_batched(const kk_bp_problem* problems, int32_t n,
+                                      void* stream);
+
 /* ---- FDK pre-processing ---------------------------------------------- */
 
 /* Cone-beam cosine pre-weighting (replaces processing.preweight,
