@@ -104,8 +104,8 @@ __device__ __forceinline__ void bp_block(const BpArgs& L, int bx, int by, int bz
         } else if (EPI == BP_UPDATE) {
             const int64_t e = vbase + i * vstep;
             float x = ld_rw(p);
-            x = __fsub_rn(x, __fmul_rn(vacc[i], __ldg(L.upd_scale + e)));
-            if (L.upd_mask) x = __fmul_rn(x, __ldg(L.upd_mask + e));
+            x = __fsub_rn(x, __fmul_rn(vacc[i], ld((const TV*)L.upd_scale + e)));
+            if (L.upd_mask) x = __fmul_rn(x, ld((const TV*)L.upd_mask + e));
             if (L.has_min) x = fmaxf(x, L.vmin);
             if (L.has_max) x = fminf(x, L.vmax);
             st(p, x);
@@ -403,7 +403,7 @@ extern "C" int kk_cone_bp_layered_update(const kk_layered* t, const kk_volume* v
                                          float out_scale, const kk_bp_update* update, float* work, void* stream) {
     const char* who = "kk_cone_bp_layered_update";
     if (!update || !update->scale) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: update scale is NULL", who);
-    if (!vol || vol->dtype != KK_F32) return kk_fail(KK_ERR_UNSUPPORTED, "%s: float32 volume only", who);
+    if (!vol) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: volume is NULL", who);
     BpArgs L;
     int rc = layered_args(L, t, vol, angles, out_scale, who);
     if (rc) return rc;
@@ -415,8 +415,15 @@ extern "C" int kk_cone_bp_layered_update(const kk_layered* t, const kk_volume* v
     L.has_max = update->has_max;
     L.work = work;
     const cudaStream_t s = (cudaStream_t)stream;
-    bp_chunks(L, true, false, true, [&](const BpArgs& c) {
-        cone_bp_kernel<float, float, true, BP_UPDATE, FETCH_TEX><<<bp_grid(c), dim3(BP_TILE_2, BP_TILE_1), 0, s>>>(c);
+    const int vdt = vol->dtype;
+    bp_chunks(L, vdt == KK_F32, false, true, [&](const BpArgs& c) {
+        const dim3 block(BP_TILE_2, BP_TILE_1);
+        if (vdt == KK_F32)
+            cone_bp_kernel<float, float, true, BP_UPDATE, FETCH_TEX><<<bp_grid(c), block, 0, s>>>(c);
+        else if (vdt == KK_BF16)
+            cone_bp_kernel<float, __nv_bfloat16, true, BP_UPDATE, FETCH_TEX><<<bp_grid(c), block, 0, s>>>(c);
+        else
+            cone_bp_kernel<float, __half, true, BP_UPDATE, FETCH_TEX><<<bp_grid(c), block, 0, s>>>(c);
     });
     return kk_check_launch(who);
 }

@@ -45,8 +45,8 @@ struct FpArgs {
     int slab;       // slices per coordinate restart
     const kk_fp_angle* angles;
     float os[9];
-    const float* res_y;
-    const float* res_w;
+    const void* res_y;  // elements of the projections' type
+    const void* res_w;
     int additive;
     int rank[3];  // memory rank of each world axis: 0 fastest .. 2 slowest
     cudaTextureObject_t vtex;  // layered texture of the volume, or 0
@@ -65,8 +65,8 @@ struct BpArgs {
     const kk_bp_angle* angles;
     float scale;
     int additive;
-    const float* upd_scale;
-    const float* upd_mask;
+    const void* upd_scale;  // elements of the volume's type
+    const void* upd_mask;
     float vmin, vmax;
     int has_min, has_max;
     cudaTextureObject_t tex;  // layered texture of the projections (FETCH_TEX)

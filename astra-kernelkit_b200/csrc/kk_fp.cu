@@ -299,7 +299,7 @@ __device__ __forceinline__ void fp_trace(const FpArgs& L, const kk_fp_angle* P, 
         if (EPI == FP_RESIDUAL) {
             const int r = r0 + lane + 32 * k;
             const int64_t e = (int64_t)a * L.ps[0] + (int64_t)r * L.ps[1] + (int64_t)c * L.ps[2];
-            out = __fmul_rn(__fsub_rn(out, __ldg(L.res_y + e)), __ldg(L.res_w + e));
+            out = __fmul_rn(__fsub_rn(out, ld((const TP*)L.res_y + e)), ld((const TP*)L.res_w + e));
         }
         st(out_ptr(k), out);
     }
@@ -402,11 +402,12 @@ static int launch_fp(const FpArgs& L, int n_angles, int vdt, int pdt, bool tex8,
         return kk_check_launch("kk_cone_fp");                         \
     }
     KK_FP_CASE(KK_F32, KK_F32, float, float)
+    // 16-bit storage (volume in bf16 or f16, projections in f16)
+    KK_FP_CASE(KK_BF16, KK_F16, __nv_bfloat16, __half)
+    KK_FP_CASE(KK_F16, KK_F16, __half, __half)
     if (EPI == FP_STORE) {
         KK_FP_CASE(KK_BF16, KK_F32, __nv_bfloat16, float)
         KK_FP_CASE(KK_F16, KK_F32, __half, float)
-        KK_FP_CASE(KK_BF16, KK_F16, __nv_bfloat16, __half)
-        KK_FP_CASE(KK_F16, KK_F16, __half, __half)
         KK_FP_CASE(KK_BF16, KK_BF16, __nv_bfloat16, __nv_bfloat16)
         KK_FP_CASE(KK_F32, KK_F16, float, __half)
         KK_FP_CASE(KK_F32, KK_BF16, float, __nv_bfloat16)
@@ -476,8 +477,7 @@ extern "C" int kk_cone_fp_residual(const kk_volume* vol, const kk_projections* o
         return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_cone_fp_residual: residual operands are NULL");
     if (out->table)
         return kk_fail(KK_ERR_UNSUPPORTED, "kk_cone_fp_residual: strided projections only");
-    if (out->dtype != KK_F32 || vol->dtype != KK_F32)
-        return kk_fail(KK_ERR_UNSUPPORTED, "kk_cone_fp_residual: float32 volume and projections only");
+
     L.res_y = residual->y;
     L.res_w = residual->weight;
     return launch_fp<FP_RESIDUAL>(L, (int)out->n_angles, vol->dtype, out->dtype, interp == KK_INTERP_TEX8,
@@ -506,8 +506,7 @@ extern "C" int kk_cone_fp_layered(const kk_layered* vtex, const kk_volume* vol, 
     if (residual) {
         if (!residual->y || !residual->weight)
             return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: residual operands are NULL", who);
-        if (proj->table || proj->dtype != KK_F32 || vol->dtype != KK_F32)
-            return kk_fail(KK_ERR_UNSUPPORTED, "%s: residual epilogue needs float32 strided data", who);
+        if (proj->table) return kk_fail(KK_ERR_UNSUPPORTED, "%s: residual epilogue needs strided data", who);
         L.res_y = residual->y;
         L.res_w = residual->weight;
         return launch_fp<FP_RESIDUAL>(L, (int)proj->n_angles, vol->dtype, proj->dtype, true, (cudaStream_t)stream);

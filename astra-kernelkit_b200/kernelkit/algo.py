@@ -126,18 +126,34 @@ class SIRT:
     def __init__(self, projections, projection_geometry,
                  volume_geometry: VolumeGeometry, mask=None,
                  min_constraint: float = None, max_constraint: float = None,
-                 interpolation: str = "texture"):
+                 interpolation: str = "texture", volume_dtype=None,
+                 projection_dtype=None):
+        """``volume_dtype`` / ``projection_dtype`` (torch dtypes, default
+        float32) choose the storage of the iterate, ``C`` and the mask, and
+        of the measured data, ``R`` and the residual: 16-bit storage
+        (``torch.bfloat16`` / ``torch.float16`` volumes, ``torch.float16``
+        projections) keeps FP32 accumulation inside every projection and
+        samples float16 textures."""
         t = _arrays.torch()
         if len(projections) != len(projection_geometry):
             raise ValueError(
                 "Number of projections does not match number of geometries.")
+        vdt = volume_dtype or t.float32
+        pdt = projection_dtype or t.float32
+        if vdt not in (t.float32, t.bfloat16, t.float16) or pdt not in (
+                t.float32, t.float16) or ((vdt == t.float32) != (pdt == t.float32)):
+            raise NotImplementedError(
+                "SIRT storage: float32 throughout, or a bfloat16/float16 "
+                "volume with float16 projections.")
+        half = vdt != t.float32
         self.vg = volume_geometry
         self.pg = projection_geometry
-        self.y = _arrays.as_tensor(projections, dtype=t.float32).contiguous()
+        self.y = _arrays.as_tensor(projections).to(pdt).contiguous()
         if self.y.dim() != 3:
             raise ValueError("Projections must be (angles, rows, cols).")
         shape = tuple(int(s) for s in volume_geometry.shape)
         self.fp = RayDrivenConeFP(interpolation=interpolation)
+        self.fp.half_texture = half
         self.fp.compile()
         self.fp.set_params(self.fp.geoms2params(projection_geometry,
                                                 volume_geometry))
@@ -145,30 +161,35 @@ class SIRT:
         self.bp.compile()
         self.bp.set_params(self.bp.geoms2params(projection_geometry,
                                                 volume_geometry))
-        self.x = t.zeros(shape, dtype=t.float32, device="cuda")
+        self.x = t.zeros(shape, dtype=vdt, device="cuda")
         self.mask = (None if mask is None
-                     else _arrays.as_tensor(mask, dtype=t.float32).contiguous())
+                     else _arrays.as_tensor(mask).to(vdt).contiguous())
         self.min_c, self.max_c = min_constraint, max_constraint
         L = _native.load()
         stream = _native.current_stream()
-        # C = 1 / A^T 1
-        self.C = t.empty(shape, dtype=t.float32, device="cuda")
-        ones = t.ones_like(self.y)
-        self.bp(ones, self.C, volume_geometry, additive=False)
-        _native.check(L.kk_reciprocal(self.C.data_ptr(), self.C.numel(),
-                                      stream))
+        # C = 1 / A^T 1 and R = 1 / A 1, formed in float32
+        C = t.empty(shape, dtype=t.float32, device="cuda")
+        ones = t.ones(self.y.shape, dtype=t.float32, device="cuda")
+        self.bp(ones, C, volume_geometry, additive=False)
+        _native.check(L.kk_reciprocal(C.data_ptr(), C.numel(), stream))
         del ones
-        # R = 1 / A 1
-        self.R = t.empty_like(self.y)
+        self.C = C if not half else C.to(vdt)
+        del C
+        R = t.empty(self.y.shape, dtype=t.float32, device="cuda")
         ones = t.ones(shape, dtype=t.float32, device="cuda")
-        self.fp(ones, self.pg, volume_geometry, self.R, additive=False)
-        _native.check(L.kk_reciprocal(self.R.data_ptr(), self.R.numel(),
-                                      stream))
+        self.fp(ones, self.pg, volume_geometry, R, additive=False)
+        _native.check(L.kk_reciprocal(R.data_ptr(), R.numel(), stream))
         del ones
+        self.R = R if not half else R.to(pdt)
+        del R
+        # make the forward projector's volume texture for the iterate's
+        # storage type now: it cannot be created during graph capture
+        self.fp._volume_texture(self.x, _native.volume_desc(self.x))
         self.y_tmp = t.empty_like(self.y)
         # the backprojection samples the residual through a layered
         # texture (the reference's filter), refilled every iteration
-        self.tex = (_native.Layered(*self.y.shape, _native.KK_F32)
+        self.tex = (_native.Layered(*self.y.shape, _native.KK_F16 if half
+                                    else _native.KK_F32)
                     if interpolation == "texture" and len(self.y) <= 2048
                     else None)
         self.bp._work_for(self.x, True)  # allocate before any graph capture

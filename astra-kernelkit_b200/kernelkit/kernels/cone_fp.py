@@ -113,6 +113,9 @@ class RayDrivenConeFP(BaseKernel):
     cuda_core_fraction = 0.0
     #: records of one ray axis launched back to back before the next axis
     axis_group = 4
+    #: let 16-bit volumes use a float16 layered texture (reduced-precision
+    #: filtering: for 16-bit storage runs, whose tolerance is the storage's)
+    half_texture = False
 
     def __init__(self, pixels_per_block: tuple = None,
                  slices_per_block: int = None,
@@ -273,21 +276,33 @@ class RayDrivenConeFP(BaseKernel):
         axis), refilled from ``vol``; None when the texture unit is not
         used for this call."""
         t = _arrays.torch()
-        # float32 only: the texture unit filters 16-bit texels in reduced
-        # precision, while the reference's arithmetic is float32
+        # The texture unit filters 16-bit texels in reduced precision while
+        # the reference's arithmetic is float32, so 16-bit volumes use a
+        # (float16) texture only when half_texture allows it, for 16-bit
+        # storage runs whose tolerance is that of the storage anyway.
+        half = vol.dtype in (t.float16, t.bfloat16)
         if (not self.use_texture_unit or self._interp != _native.KK_INTERP_TEX8
-                or vol.dtype != t.float32
+                or (half and not self.half_texture)
+                or vol.dtype not in (t.float32, t.float16, t.bfloat16)
                 or not vol.is_contiguous() or vol.shape[0] > 2048):
             return None
         slowest = self._vol_axs[0]
         if not np.any(self._host_params["axis"] == slowest):
             return None
-        code = _native.dtype_code(vol)
+        code = _native.KK_F16 if half else _native.KK_F32
         lay = self._vtex
         if lay is None or lay.shape != tuple(vol.shape) or lay.dtype != code:
             lay = _native.Layered(*vol.shape, code)
             self._vtex = lay
-        lay.copy_from(vol)
+        src = vol
+        if vol.dtype == t.bfloat16:  # texels are float16: convert first
+            stage = getattr(self, "_half_stage", None)
+            if stage is None or stage.shape != vol.shape:
+                stage = t.empty(vol.shape, dtype=t.float16, device=vol.device)
+                self._half_stage = stage
+            stage.copy_(vol)
+            src = stage
+        lay.copy_from(src)
         return lay
 
     # -- launch -------------------------------------------------------------

@@ -98,19 +98,19 @@ typedef struct {
 
 /* Optional fused epilogue of the forward projection (SIRT residual step,
  * reference algo.py:339-344): out = (A x - y) * weight, elementwise in the
- * layout of `out`. y and weight are float32 and share out's strides. */
+ * layout of `out`. y and weight have out's element type and strides. */
 typedef struct {
-    const float* y;
-    const float* weight;
+    const void* y;
+    const void* weight;
 } kk_fp_residual;
 
 /* Optional fused epilogue of the backprojection (SIRT update, reference
  * algo.py:356-362): x = clip(mask * (x - scale * A^T r)), in place on the
- * volume passed to kk_cone_bp_update. scale/mask are float32 with the
- * volume's strides; mask may be NULL. */
+ * volume passed to kk_cone_bp_update. scale/mask have the volume's element
+ * type and strides; mask may be NULL. */
 typedef struct {
-    const float* scale;
-    const float* mask;
+    const void* scale;
+    const void* mask;
     float min_value;
     float max_value;
     int32_t has_min;
