@@ -400,6 +400,101 @@ def run_batched(n_problems=32, iters=30, seed=1237):
             "autotuned": {"fp_axis_group": sorted(set(tuner.cache.values()))}}
 
 
+def run_sirt_config5(iters=20, seed=1239):
+    """Config 5: 20 SIRT iterations at 1024^3 voxels / 1440 angles /
+    1536^2 detector (SOD 3000, SDD 6000, pitch 1), plain float32 storage
+    against a bfloat16 volume with float16 projections (FP32 accumulation,
+    float16 textures). Data: the float32 forward projection of a voxelised
+    200-ellipsoid phantom. Reported per storage: it/s (CUDA events around
+    graph replays), one FP and one BP time, the reconstruction's rel. L2 to
+    the phantom on the central 128^3 voxels, and the rel. L2 of A x_rec
+    against the exact FP64 line integrals of the phantom on 16 angles."""
+    import torch
+
+    import kernelkit as kk
+    from kernelkit import phantom
+    from kernelkit.algo import SIRT
+    from kernelkit.kernels import RayDrivenConeFP, VoxelDrivenConeBP
+
+    n, na, det_n = 1024, 1440, 1536
+    det = kk.Detector(rows=det_n, cols=det_n, pixel_height=1.0,
+                      pixel_width=1.0)
+    g0 = kk.ProjectionGeometry([-3000.0, 0.0, 0.0], [3000.0, 0.0, 0.0], det)
+    pgs = [kk.rotate(g0, yaw=2 * np.pi * k / na) for k in range(na)]
+    vg = kk.resolve_volume_geometry(shape=n, voxel_size=1.0)
+    ell = phantom.random_ellipsoids(200, 384.0, (32.0, 320.0), seed=seed)
+    truth = phantom.voxelize_torch(ell, vg.shape, vg.extent_min,
+                                   vg.voxel_size, device="cuda")
+    fp = RayDrivenConeFP()
+    fp.compile()
+    fp.set_params(fp.geoms2params(pgs, vg))
+    y = torch.empty((na, det_n, det_n), device="cuda")
+    fp(truth, pgs, vg, y, additive=False)
+    sel = list(range(0, na, na // 16))[:16]
+    srcs, pixs = phantom.pixel_centres([pgs[i] for i in sel])
+    exact = phantom.line_integrals(ell, srcs, pixs, device="cuda")
+    c = slice(n // 2 - 64, n // 2 + 64)
+    tc = truth[c, c, c].double()
+    fsub = RayDrivenConeFP()
+    fsub.compile()
+    fsub.set_params(fsub.geoms2params([pgs[i] for i in sel], vg))
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b)
+
+    out = {}
+    for name, vdt, pdt in (("fp32", None, None),
+                           ("bf16_volume_f16_projections", torch.bfloat16,
+                            torch.float16)):
+        s = SIRT(y, pgs, vg, volume_dtype=vdt, projection_dtype=pdt)
+        s.capture()
+        ms = timed(lambda: s.run(iters, use_graph=True))
+        x = s.x
+        # one forward projection and one backprojection in this storage
+        f = RayDrivenConeFP()
+        f.half_texture = vdt is not None
+        f.compile()
+        f.set_params(f.geoms2params(pgs, vg))
+        t_fp = timed(lambda: f(x, pgs, vg, s.y_tmp, additive=False))
+        bp = VoxelDrivenConeBP()
+        bp.compile()
+        bp.set_params(bp.geoms2params(pgs, vg))
+        s.tex.copy_from(s.y_tmp)
+        tmpv = torch.empty_like(x)
+        t_bp = timed(lambda: bp(s.tex, tmpv, vg, additive=False))
+        del tmpv, f, bp
+        xs = x.float()
+        sub = torch.empty((16, det_n, det_n), device="cuda")
+        fsub(xs, [pgs[i] for i in sel], vg, sub, additive=False)
+        out[name] = {
+            "it_per_s": iters / (ms * 1e-3), "ms_per_iter": ms / iters,
+            "fp_ms": t_fp, "bp_ms": t_bp,
+            "rel_l2_phantom_center128": float(
+                (xs[c, c, c].double() - tc).norm() / tc.norm()),
+            "rel_l2_projections_vs_fp64_16_angles": float(
+                (sub.double() - exact).norm() / exact.norm()),
+            "storage": {"volume": str(x.dtype).replace("torch.", ""),
+                        "projections": str(s.y.dtype).replace("torch.", "")}}
+        if name == "fp32":
+            x32 = xs.clone()
+        else:
+            out[name]["rel_l2_to_fp32_reconstruction"] = float(
+                (xs - x32).norm() / x32.norm())
+        del s, x, xs, sub
+        torch.cuda.empty_cache()
+    out["speedup_16bit_over_fp32"] = (
+        out["bf16_volume_f16_projections"]["it_per_s"] / out["fp32"]["it_per_s"])
+    return {"metric": "SIRT it/s @1024^3/1440 ang, 16-bit storage vs fp32",
+            "workload": "config5", "iters": iters, **out}
+
+
 def run_ours(args):
     import torch
 
@@ -605,10 +700,16 @@ def main(argv=None):
                     default="headline")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sirt-config5", action="store_true",
+                    help="only run the 1024^3 SIRT storage comparison "
+                         "(several minutes; prints its own JSON line)")
     ap.add_argument("--no-sirt", action="store_true",
                     help="skip the SIRT measurements (config 2 and the "
                          "batched config 4)")
     args = ap.parse_args(argv)
+    if args.sirt_config5:
+        print(json.dumps(run_sirt_config5()), flush=True)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
