@@ -2,6 +2,13 @@
 // projection textures and the kk_cone_bp* entry points of include/kk.h.
 #include <mutex>
 
+#ifndef KK_BP_LANES
+#define KK_BP_LANES 1  // 2 x 2 quads of lanes (0: lanes along the fastest axis)
+#endif
+#ifndef KK_BP_WZ
+#define KK_BP_WZ 16  // voxels per warp along the fastest axis
+#endif
+
 #include "kk_cone.cuh"
 
 namespace kk {
@@ -18,8 +25,19 @@ __device__ __forceinline__ void bp_block(const BpArgs& L, int bx, int by, int bz
     // running sum vol += acc * scale is carried between launches in the
     // volume (float32) or in the float32 work buffer.
     __shared__ kk_bp_angle sp[BP_CHUNK];
+#if KK_BP_LANES == 0
     const int i2 = bx * BP_TILE_2 + threadIdx.x;
     const int i1 = by * BP_TILE_1 + threadIdx.y;
+#else
+    // warps cover KK_BP_WZ (fastest axis) x 32 / KK_BP_WZ (middle axis)
+    // voxels, and every quad of lanes a 2 x 2 square of them
+    const int lane = threadIdx.x, w = threadIdx.y;
+    constexpr int WZ = KK_BP_WZ, WY = 32 / WZ;
+    const int zl = (lane & 1) | (((lane >> 2) * 2) % WZ);
+    const int yl = ((lane >> 1) & 1) | ((((lane >> 2) * 2) / WZ) * 2);
+    const int i2 = bx * BP_TILE_2 + (w % (BP_TILE_2 / WZ)) * WZ + zl;
+    const int i1 = by * BP_TILE_1 + (w / (BP_TILE_2 / WZ)) * WY + yl;
+#endif
     const int g0 = bz * BP_GROUP;
     const int n0 = L.vn[L.m0], n1 = L.vn[L.m1], n2 = L.vn[L.m2];
     const bool active = i2 < n2 && i1 < n1;
