@@ -239,12 +239,22 @@ def dist_setup():
 
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(
-            seconds=120), device_id=torch.device("cuda", local))
-    else:
+        timeout = datetime.timedelta(seconds=120)
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=timeout,
+                                    device_id=torch.device("cuda", local))
+        else:  # host-only runs of the replica logic
+            dist.init_process_group("gloo", timeout=timeout)
+    elif torch.cuda.is_available():
         torch.cuda.set_device(0)
     return rank, world, local
+
+
+def _reduce_device():
+    import torch.distributed as dist
+
+    return "cuda" if dist.get_backend() == "nccl" else "cpu"
 
 
 def max_over_ranks(x, world):
@@ -253,7 +263,7 @@ def max_over_ranks(x, world):
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_reduce_device())
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -265,7 +275,8 @@ def barrier(world):
         import torch.distributed as dist
 
         dist.barrier()
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
 
 
 def load_peaks():

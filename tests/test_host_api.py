@@ -146,3 +146,19 @@ def test_phantom_sphere_line_integral():
     assert np.isclose(li[0, 0, 1], 0.5 * 2 * np.sqrt(25 - d * d))
     vol = phantom.voxelize(ell, (20, 20, 20), (-10, -10, -10), (1, 1, 1))
     assert np.isclose(vol.sum() * 1.0, 0.5 * 4 / 3 * np.pi * 125, rtol=0.1)
+
+
+def test_autotuner_reuses_its_json_cache(tmp_path):
+    """A cached choice is returned without timing anything (the timing
+    itself needs a GPU and is covered by the GPU batch tests)."""
+    import json
+
+    from kernelkit.batch import Autotuner
+
+    path = tmp_path / "tune.json"
+    path.write_text(json.dumps({"fp_axis_group:[[8,8,8],6,[9,9]]": 2}))
+    tuner = Autotuner(str(path))
+    calls = []
+    assert tuner.pick("fp_axis_group:[[8,8,8],6,[9,9]]", (1, 2, 4),
+                      calls.append) == 2
+    assert calls == []
