@@ -90,6 +90,30 @@ __global__ void fpt_rays_kernel(const FptArgs L) {
     L.ray_pc[id] = p * (R.corr * L.os[3 * A + 2]);
 }
 
+// A ray's in-slice coordinate at slice off + nst: the slab-start value v0
+// followed by nst rounded adds of the slope, exactly as the forward
+// projector computes it. With texture-compatible weights the split only
+// sees floor(256 v - 127.5); each rounded add errs by at most half an ulp
+// (2^-24 relative), so the sequence ends within eps of fma(nst, a, v0), and
+// when no boundary of floor() lies within eps of that direct value (for
+// |v| < 2^13, q = 256 v - 127.5 and q - floor(q) are exact in float32) it
+// splits exactly as the sequence would and is returned instead.
+template <bool TEX8>
+__device__ __forceinline__ float slice_coord(float v0, float a, int nst) {
+    if (TEX8) {
+        const float fn = (float)nst;
+        const float vd = fmaf(fn, a, v0);
+        const float eps = (fn + 1.f) * 1.2e-7f * (fabsf(vd) + fabsf(a) * fn + 1.f);
+        const float q = 256.f * vd - 127.5f;
+        const float f = q - floorf(q);
+        const float e = 256.f * 1.01f * eps + 1e-6f;
+        if (fabsf(vd) < 8192.f && f > e && f < 1.f - e) return vd;
+    }
+    float v = v0;
+    for (int q = 0; q < nst; ++q) v = __fadd_rn(v, a);
+    return v;
+}
+
 template <bool TEX8>
 __global__ void __launch_bounds__(FPT_TILE_2* FPT_TILE_1) fpt_gather_kernel(const FptArgs L) {
     const int i2 = blockIdx.x * FPT_TILE_2 + threadIdx.x;
@@ -186,54 +210,26 @@ __global__ void __launch_bounds__(FPT_TILE_2* FPT_TILE_1) fpt_gather_kernel(cons
         const float vA = A == 0 ? v[0] : (A == 1 ? v[1] : v[2]);
         const float vD1 = D1 == 0 ? v[0] : v[1];
         const bool shared = vA == 0.f && vD1 == 0.f;
+        const int nst = s - off;
         for (int c = c0; c <= c1; ++c) {
+            // shared case: one D1 coordinate for the whole column
+            Split syc;
+            bool col = false;
             if (shared && rlo <= rhi) {
                 const float4 ab = __ldg(&L.ray_ab[(int64_t)k * per + (int64_t)c * L.rows + rlo]);
-                float y = __fadd_rn(fmaf(ab.x, t1, ab.y), half1);
-                for (int q = off; q < s; ++q) y = __fadd_rn(y, ab.x);
-                const int di = jv - split_coord<TEX8>(y).i;
-                if ((unsigned)di > 1u) continue;
+                syc = split_coord<TEX8>(slice_coord<TEX8>(__fadd_rn(fmaf(ab.x, t1, ab.y), half1), ab.x, nst));
+                if ((unsigned)(jv - syc.i) > 1u) continue;
+                col = true;
             }
             for (int r = rlo; r <= rhi; ++r) {
                 const int64_t id = (int64_t)k * per + (int64_t)c * L.rows + r;
                 const float4 ab = __ldg(&L.ray_ab[id]);
-                // the forward projector's coordinate sequence for slice s:
-                // the slab-start value, then one rounded add per slice
-                float y = __fadd_rn(fmaf(ab.x, t1, ab.y), half1);
-                float z = __fadd_rn(fmaf(ab.z, t1, ab.w), half2);
-                bool chain = true;
-                if (TEX8) {
-                    // The texture-compatible split only sees
-                    // floor(256 y - 127.5). Each of the nst rounded adds
-                    // errs by at most half an ulp (2^-24 relative), so the
-                    // chain ends within eps of fma(nst, a, y0); when no
-                    // boundary of floor() lies within that distance, the
-                    // direct value splits exactly as the chain would.
-                    const float nst = (float)(s - off);
-                    const float yd = fmaf(nst, ab.x, y), zd = fmaf(nst, ab.z, z);
-                    const float eps = (nst + 1.f) * 1.2e-7f * (fmaxf(fabsf(yd), fabsf(zd)) + fabsf(ab.x) * nst +
-                                                                  fabsf(ab.z) * nst + 1.f);
-                    // for |y| < 2^13, q = 256 y - 127.5 and q - floor(q)
-                    // are exact in float32, so the distance to the next
-                    // boundary is known exactly
-                    const float qy = 256.f * yd - 127.5f, qz = 256.f * zd - 127.5f;
-                    const float fy = qy - floorf(qy), fz = qz - floorf(qz);
-                    const float e = 256.f * 1.01f * eps + 1e-6f;
-                    if (fabsf(yd) < 8192.f && fabsf(zd) < 8192.f && fy > e && fy < 1.f - e && fz > e &&
-                        fz < 1.f - e) {
-                        y = yd;
-                        z = zd;
-                        chain = false;
-                    }
-                }
-                if (chain) {
-                    for (int q = off; q < s; ++q) {
-                        y = __fadd_rn(y, ab.x);
-                        z = __fadd_rn(z, ab.z);
-                    }
-                }
-                const Split sy = split_coord<TEX8>(y);
-                const Split sz = split_coord<TEX8>(z);
+                // the forward projector's coordinates for slice s
+                const Split sy =
+                    col ? syc
+                        : split_coord<TEX8>(slice_coord<TEX8>(__fadd_rn(fmaf(ab.x, t1, ab.y), half1), ab.x, nst));
+                const Split sz =
+                    split_coord<TEX8>(slice_coord<TEX8>(__fadd_rn(fmaf(ab.z, t1, ab.w), half2), ab.z, nst));
                 const int di = jv - sy.i, dj = kv - sz.i;
                 if ((unsigned)di > 1u || (unsigned)dj > 1u) continue;
                 const W4 wt = weights4<TEX8>(sy.w, sz.w, rule, a_fast);
