@@ -36,6 +36,9 @@ for _p in (ROOT, os.path.join(ROOT, "astra-kernelkit_b200")):
 import numpy as np  # noqa: E402
 
 METRIC = "cone FP+BP GUPS @512^3/720 ang"
+#: float32 2D-layered bilinear fetches per clock per SM of the B200's
+#: texture unit (astra-kernelkit_b200/csrc/probes/tex_rate.cu)
+TMU_FETCH_PER_CLK_SM = 3.83
 UNIT = "GUPS"
 
 WORKLOADS = {
@@ -706,6 +709,22 @@ def run_ours(args):
                 "peak_kind": peak_kind,
                 "traffic": load_traffic(args.workload, "cone_fp_kernel"),
                 "algorithmic_bytes_per_launch": fp_bytes}
+    # The backprojector samples one bilinear texel quad per update; its
+    # ceiling is the texture unit's fetch rate, measured on this GPU model
+    # with astra-kernelkit_b200/csrc/probes/tex_rate.cu (3.83 float32
+    # bilinear fetches per clock per SM), at the SM clock seen during the
+    # timed region.
+    sm_hz = 1e6 * float(clocks.get("sm_mhz") or clocks.get("sm_max_mhz")
+                        or 1965.0)
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    tmu_peak = TMU_FETCH_PER_CLK_SM * sms * sm_hz
+    texture_roofline = {
+        "kernel": "cone_bp_kernel", "bound": "texture unit",
+        "achieved": nupd / (t_bp * 1e-3), "peak": tmu_peak,
+        "unit": "bilinear fetches/s",
+        "frac": nupd / (t_bp * 1e-3) / tmu_peak,
+        "peak_source": f"{TMU_FETCH_PER_CLK_SM} fetches/clk/SM measured "
+                       "(csrc/probes/tex_rate.cu) x SMs x SM clock"}
     kernels = {
         # "traffic": ncu DRAM bytes per launch (profiles/), "ms": all
         # launches of one operator application
@@ -745,7 +764,8 @@ def run_ours(args):
                        "l2": "inputs larger than L2 (volume 537 MB, "
                              "sinogram 1.7 GB), no flush",
                        "parallelism": f"replicas x{world}"},
-            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+            "e2e": e2e, "roofline": roofline,
+            "texture_roofline": texture_roofline, "cpu_baseline": cpu,
             "kernels": kernels,
             # per step: one FP launch and one BP launch per 32-angle chunk
             "gpu_launches": args.steps * (1 + (len(pgs) + 31) // 32),
