@@ -2,6 +2,8 @@
 // row filtering, both in float64 as the reference evaluates them
 // (processing.py:96-126, 149-188), plus the SIRT reciprocal helper.
 #include <cuda_runtime.h>
+
+#include <algorithm>
 #include <stdint.h>
 
 #include "kk_common.cuh"
@@ -10,7 +12,7 @@ namespace kk {
 
 constexpr int PW_BLOCK = 256;
 constexpr int FILT_BLOCK = 256;
-constexpr int FILT_MAX_COLS = 8192;
+constexpr int FILT_MAX_COLS = 8192;  // 24 cols + 64 bytes of shared memory per block
 
 // p *= |d - s| / |pixel - s|; pixel = corner + col * u_pw + row * v_ph.
 // Evaluated with the operation order of processing.py:182-186 and of
@@ -37,26 +39,54 @@ __global__ void __launch_bounds__(PW_BLOCK)
     *e = __double2float_rn(__dmul_rn((double)*e, w));
 }
 
-// out[i] = sum_j p[j] * h[(i - j) mod P] for one detector row; the row is
-// staged in shared memory as float64, h is read through the read-only
-// cache.
+// out[i] = sum_j p[j] * h[(i - j) mod P] for one detector row (j ascending,
+// one float64 fma per term). The row is staged in shared memory as float64,
+// together with hx[m] = h[(m - cols) mod P], so that term (i, j) reads
+// hx[i - j + cols] without a wrap test. Each thread produces four
+// consecutive outputs i0..i0+3; their filter taps at step j are
+// hx[i0 + cols - j + q], so going from j to j + 1 shifts the four taps by
+// one and a single new tap is read (a sliding window in registers). hx is
+// stored as four interleaved sub-arrays (index m at [m % 4][m / 4]) so the
+// lanes of a warp, whose windows start four taps apart, read consecutive
+// doubles of one sub-array: no bank conflicts.
 __global__ void __launch_bounds__(FILT_BLOCK)
     filter_rows_kernel(float* data, const uint64_t* table, int64_t sa, int64_t sr, int64_t sc, int rows, int cols,
                        const double* __restrict__ h, int P) {
-    extern __shared__ double row[];
+    extern __shared__ double sm[];
+    double* row = sm;
+    const int HN = 2 * cols + 8;
+    const int HQ = (HN + 3) / 4;
+    double* H = sm + cols;
     const int line = blockIdx.x;
     const int a = line / rows, r = line % rows;
     float* base = (table ? (float*)table[a] : data + (int64_t)a * sa) + (int64_t)r * sr;
-    for (int j = threadIdx.x; j < cols; j += FILT_BLOCK) row[j] = (double)base[(int64_t)j * sc];
+    for (int j = threadIdx.x; j < cols; j += blockDim.x) row[j] = (double)base[(int64_t)j * sc];
+    for (int m = threadIdx.x; m < HN; m += blockDim.x) H[(m & 3) * HQ + (m >> 2)] = __ldg(h + (m - cols + P) % P);
     __syncthreads();
-    for (int i = threadIdx.x; i < cols; i += FILT_BLOCK) {
-        double acc = 0.0;
+    for (int i0 = 4 * threadIdx.x; i0 < cols; i0 += 4 * blockDim.x) {
+        const int b = i0 + cols;
+        double h0 = H[(b & 3) * HQ + (b >> 2)];
+        double h1 = H[((b + 1) & 3) * HQ + ((b + 1) >> 2)];
+        double h2 = H[((b + 2) & 3) * HQ + ((b + 2) >> 2)];
+        double h3 = H[((b + 3) & 3) * HQ + ((b + 3) >> 2)];
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+#pragma unroll 4
         for (int j = 0; j < cols; ++j) {
-            int k = i - j;
-            k += (k < 0) ? P : 0;
-            acc = fma(row[j], __ldg(h + k), acc);
+            const double x = row[j];
+            a0 = fma(x, h0, a0);
+            a1 = fma(x, h1, a1);
+            a2 = fma(x, h2, a2);
+            a3 = fma(x, h3, a3);
+            const int n = b - j - 1;  // >= i0 >= 0
+            h3 = h2;
+            h2 = h1;
+            h1 = h0;
+            h0 = H[(n & 3) * HQ + (n >> 2)];
         }
-        base[(int64_t)i * sc] = __double2float_rn(acc);
+        const double acc[4] = {a0, a1, a2, a3};
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (i0 + q < cols) base[(int64_t)(i0 + q) * sc] = __double2float_rn(acc[q]);
     }
 }
 
@@ -105,14 +135,17 @@ extern "C" int kk_filter_rows(const kk_projections* proj, const double* h, int64
                        (long long)P);
     const int64_t lines = proj->n_angles * proj->rows;
     if (lines > 0x7fffffff) return kk_fail(KK_ERR_UNSUPPORTED, "kk_filter_rows: too many rows");
-    const size_t smem = sizeof(double) * (size_t)proj->cols;
+    // the row and the four interleaved copies of hx (2 cols + 8 taps)
+    const int64_t hq = (2 * proj->cols + 8 + 3) / 4;
+    const size_t smem = sizeof(double) * (size_t)(proj->cols + 4 * hq);
     static bool attr_set = false;
     if (!attr_set) {
         cudaFuncSetAttribute(filter_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(sizeof(double) * FILT_MAX_COLS));
+                             (int)(sizeof(double) * (FILT_MAX_COLS + 4 * ((2 * FILT_MAX_COLS + 11) / 4))));
         attr_set = true;
     }
-    filter_rows_kernel<<<(unsigned)lines, FILT_BLOCK, smem, (cudaStream_t)stream>>>(
+    const int threads = (int)std::min<int64_t>(FILT_BLOCK, ((proj->cols + 3) / 4 + 31) / 32 * 32);
+    filter_rows_kernel<<<(unsigned)lines, threads, smem, (cudaStream_t)stream>>>(
         (float*)proj->data, proj->table, proj->stride[0], proj->stride[1], proj->stride[2], (int)proj->rows,
         (int)proj->cols, h, (int)P);
     return kk_check_launch("kk_filter_rows");

@@ -25,8 +25,18 @@ from .processing import preweight
 from .projector import BackProjector
 
 
+def _host_copy(dev):
+    """A host copy of a device tensor in pinned memory, as the reference
+    returns its results (``algo.py:46-48, 122-126``): the copy runs at
+    full bus speed and torch's host allocator reuses the pinned block."""
+    t = _arrays.torch()
+    host = t.empty(dev.shape, dtype=dev.dtype, pin_memory=True)
+    host.copy_(dev)
+    return host.numpy()
+
+
 def _to_host(dev, out=None):
-    host = dev.cpu().numpy() if out is None else None
+    host = _host_copy(dev) if out is None else None
     if out is None:
         return host
     if isinstance(out, np.ndarray):
@@ -85,7 +95,7 @@ def bp(projections: Any, projection_geometry, volume_geometry: VolumeGeometry,
     if isinstance(out, np.ndarray):
         out[...] = out_gpu.cpu().numpy()
         return out
-    return out_gpu.cpu().numpy()
+    return _host_copy(out_gpu)
 
 
 def fbp(projections: Any, projection_geometry, volume_geometry,
@@ -276,7 +286,7 @@ def sirt(projections: np.ndarray, projection_geometry: Any,
         bar.close()
     if return_gpu:
         return x
-    return x.cpu().numpy()
+    return _host_copy(x)
 
 
 __all__ = ["fp", "bp", "fbp", "fdk", "sirt", "SIRT"]
