@@ -748,8 +748,18 @@ def run_ours(args):
                "sample": desc, "seconds": secs}
     sirt = batched = None
     if rank == 0 and world == 1 and not args.no_sirt:
-        sirt = run_sirt("config2", 50)
-        batched = run_batched()
+        # secondary measurements: a failure here is reported in the line
+        # instead of costing the headline number
+        for name, fn in (("sirt", lambda: run_sirt("config2", 50)),
+                         ("batched", run_batched)):
+            try:
+                res = fn()
+            except Exception as e:  # noqa: BLE001
+                res = {"error": f"{type(e).__name__}: {e}"[:300]}
+            if name == "sirt":
+                sirt = res
+            else:
+                batched = res
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
