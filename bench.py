@@ -742,10 +742,14 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = len(os.sched_getaffinity(0))
-        gups, desc, secs = cpu_sample(w, pgs, vg, vol.cpu().numpy(), cores,
-                                      fp_rows=48, bp_slab=24)
-        cpu = {"value": gups, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": desc, "seconds": secs}
+        try:
+            gups, desc, secs = cpu_sample(w, pgs, vg, vol.cpu().numpy(),
+                                          cores, fp_rows=48, bp_slab=24)
+            cpu = {"value": gups, "unit": UNIT, "cores": cores,
+                   "kind": "port", "sample": desc, "seconds": secs}
+        except Exception as e:  # noqa: BLE001
+            cpu = {"value": None, "unit": UNIT, "cores": cores,
+                   "kind": "port", "error": f"{type(e).__name__}: {e}"[:300]}
     sirt = batched = None
     if rank == 0 and world == 1 and not args.no_sirt:
         # secondary measurements: a failure here is reported in the line
