@@ -90,6 +90,21 @@ __global__ void __launch_bounds__(FILT_BLOCK)
     }
 }
 
+// x = clip(mask * (x - scale * g)) elementwise (the SIRT update of
+// algo.py:356-362 once the backprojection g is complete, e.g. summed over
+// the ranks of an angle-sharded solve).
+__global__ void sirt_update_kernel(float* x, const float* __restrict__ g, const float* __restrict__ scale,
+                                   const float* __restrict__ mask, float vmin, float vmax, int has_min, int has_max,
+                                   int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        float v = __fsub_rn(x[i], __fmul_rn(g[i], scale[i]));
+        if (mask) v = __fmul_rn(v, mask[i]);
+        if (has_min) v = fmaxf(v, vmin);
+        if (has_max) v = fminf(v, vmax);
+        x[i] = v;
+    }
+}
+
 __global__ void reciprocal_kernel(float* x, int64_t n) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const float v = __fdiv_rn(1.f, x[i]);
@@ -158,4 +173,15 @@ extern "C" int kk_reciprocal(float* data, int64_t n, void* stream) {
     if (blocks > 148 * 32) blocks = 148 * 32;
     reciprocal_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(data, n);
     return kk_check_launch("kk_reciprocal");
+}
+
+extern "C" int kk_sirt_update(float* x, const float* g, const float* scale, const float* mask, float min_value,
+                              float max_value, int32_t has_min, int32_t has_max, int64_t n, void* stream) {
+    if (!x || !g || !scale || n < 0) return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_sirt_update: bad arguments");
+    if (n == 0) return KK_OK;
+    int64_t blocks = (n + 255) / 256;
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    sirt_update_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(x, g, scale, mask, min_value, max_value,
+                                                                         has_min, has_max, n);
+    return kk_check_launch("kk_sirt_update");
 }

@@ -24,6 +24,7 @@ from . import kernels  # noqa: E402,F401
 from . import experimental  # noqa: E402,F401
 from . import processing  # noqa: E402,F401
 from . import batch  # noqa: E402,F401
+from . import distributed  # noqa: E402,F401
 from .kernels import RayDrivenConeFP, VoxelDrivenConeBP  # noqa: E402,F401
 from .projector import (ProjectionGeometryNotSetError,  # noqa: E402,F401
                         VolumeGeometryNotSetError, VolumeNotSetError,

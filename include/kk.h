@@ -296,6 +296,15 @@ KK_API int kk_filter_rows(const kk_projections* proj, const double* h, int64_t P
 
 /* ---- elementwise helpers -------------------------------------------- */
 
+/* x = clip(mask * (x - scale * g)) over n dense float32 elements: the
+ * SIRT update (algo.py:356-362) applied after the backprojection g is
+ * complete, as in an angle-sharded solve where g is summed over ranks
+ * first. mask may be NULL; clipping per has_min / has_max. */
+KK_API int kk_sirt_update(float* x, const float* g, const float* scale,
+                          const float* mask, float min_value, float max_value,
+                          int32_t has_min, int32_t has_max, int64_t n,
+                          void* stream);
+
 /* x = 1 / x with +inf mapped to 0 (SIRT scaling, algo.py:320-333). */
 KK_API int kk_reciprocal(float* data, int64_t n, void* stream);
 
