@@ -668,36 +668,74 @@ def run_ours(args):
     e2e = None
     if not args.no_e2e:
         op = XrayTransform(pgs, vg)
+        # Double-buffered: step k's input copy and step k-1's result copy
+        # run on copy streams while step k-1 / k computes. Every step still
+        # moves its whole input in and its whole result out; the copies
+        # only leave the critical path.
         host_in = torch.empty(shape, dtype=torch.float32, pin_memory=True)
         host_in.copy_(vol.cpu())
-        host_out = torch.empty(shape, dtype=torch.float32, pin_memory=True)
-        dev_in = torch.empty(shape, device="cuda")
+        host_out = [torch.empty(shape, dtype=torch.float32, pin_memory=True)
+                    for _ in range(2)]
+        dev_in = [torch.empty(shape, device="cuda") for _ in range(2)]
         dev_y = torch.empty((len(pgs), w["det"], w["det"]), device="cuda")
-        dev_out = torch.empty(shape, device="cuda")
+        dev_out = [torch.empty(shape, device="cuda") for _ in range(2)]
+        s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
 
-        def e2e_step():
-            dev_in.copy_(host_in, non_blocking=True)
-            op(dev_in, out=dev_y)
-            op.T(dev_y, out=dev_out)
-            host_out.copy_(dev_out, non_blocking=True)
+        def ev():
+            return torch.cuda.Event()
 
-        for _ in range(max(1, args.warmup)):
-            e2e_step()
+        def e2e_run(n):
+            """n steps; returns after queueing them (all streams joined
+            into the current stream)."""
+            read_done = [None, None]   # compute finished reading dev_in[b]
+            out_free = [None, None]    # D2H finished reading dev_out[b]
+            s_in.wait_stream(stream)
+            s_out.wait_stream(stream)
+            for k in range(n):
+                b = k & 1
+                with torch.cuda.stream(s_in):
+                    if read_done[b] is not None:
+                        s_in.wait_event(read_done[b])
+                    dev_in[b].copy_(host_in, non_blocking=True)
+                    landed = ev()
+                    landed.record(s_in)
+                stream.wait_event(landed)
+                if out_free[b] is not None:
+                    stream.wait_event(out_free[b])
+                op(dev_in[b], out=dev_y)
+                read_done[b] = ev()
+                read_done[b].record(stream)
+                op.T(dev_y, out=dev_out[b])
+                done = ev()
+                done.record(stream)
+                with torch.cuda.stream(s_out):
+                    s_out.wait_event(done)
+                    host_out[b].copy_(dev_out[b], non_blocking=True)
+                    out_free[b] = ev()
+                    out_free[b].record(s_out)
+            stream.wait_stream(s_in)
+            stream.wait_stream(s_out)
+
+        e2e_run(max(1, args.warmup))
         barrier(world)
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        for _ in range(args.steps):
-            e2e_step()
+        e2e_run(args.steps)
         b.record(stream)
         barrier(world)
+        torch.cuda.synchronize()
         e2e_ms = max_over_ranks(a.elapsed_time(b) / args.steps, world)
+        got = host_out[(args.steps - 1) & 1]
         e2e = {"value": world * 2 * nupd / (e2e_ms * 1e-3) / 1e9,
                "unit": UNIT, "ms_per_step": e2e_ms,
                "h2d_bytes_per_step": host_in.numel() * 4,
-               "d2h_bytes_per_step": host_out.numel() * 4,
+               "d2h_bytes_per_step": got.numel() * 4,
+               "result_checksum": float(got.double().sum()),
                "path": "XrayTransform: pinned host x -> A x -> A^T (A x) -> "
-                       "pinned host"}
+                       "pinned host; input and result copies on two copy "
+                       "streams, double-buffered, overlapping the "
+                       "neighbouring steps' compute"}
         del dev_in, dev_y, dev_out
 
     peak, peak_kind = load_peaks()
