@@ -61,15 +61,181 @@ def fp(volume: Any, projection_geometry, volume_geometry: VolumeGeometry,
     return _to_host(result, out)
 
 
+#: angles per streamed chunk: the backprojector's own summation chunk, so
+#: chunked and whole-scan backprojections add in the same order
+_CHUNK = 32
+_STREAM: dict = {}
+
+
+def _stream_buffers(rows: int, cols: int) -> dict:
+    """Two-slot ring of pinned staging blocks, device blocks and 32-layer
+    textures for streaming host projections, kept for the most recent
+    detector shape (about 6 x 75 MB at 768^2)."""
+    t = _arrays.torch()
+    key = (rows, cols)
+    st = _STREAM.get(key)
+    if st is None:
+        _STREAM.clear()
+        shape = (_CHUNK, rows, cols)
+        st = {"host": [t.empty(shape, dtype=t.float32, pin_memory=True)
+                       for _ in range(2)],
+              "dev": [t.empty(shape, dtype=t.float32, device="cuda")
+                      for _ in range(2)],
+              "tex": {},  # layers -> two textures
+              "copy": t.cuda.Stream()}
+        _STREAM[key] = st
+    return st
+
+
+def _can_stream(projections, projection_geometry, volume_geometry, preproc_fn,
+                kernel, out, projection_axes, kwargs) -> bool:
+    """The chunked path takes host (NumPy) projections, or a C-contiguous
+    float32 device array, in the default layout with the default
+    backprojector; anything else goes through the general path."""
+    if isinstance(projections, np.ndarray):
+        if (projections.ndim != 3 or not projections.dtype.isnative
+                or not np.issubdtype(projections.dtype, np.floating)
+                or any(s < 0 for s in projections.strides)):
+            return False
+    elif _arrays.is_device_array(projections):
+        t = _arrays.torch()
+        d = _arrays.as_tensor(projections)
+        if d.dim() != 3 or d.dtype != t.float32 or not d.is_contiguous():
+            return False
+    else:
+        return False
+    if preproc_fn is not None or kwargs:
+        return False
+    if kernel is not None and not (
+            type(kernel) is VoxelDrivenConeBP
+            and kernel._interp == _native.KK_INTERP_TEX8
+            and tuple(kernel._vol_axs) == (0, 1, 2)
+            and tuple(kernel._proj_axs) == (0, 1, 2)):
+        return False
+    if tuple(projection_axes) != (0, 1, 2):
+        return False
+    if out is not None and not isinstance(out, np.ndarray):
+        return False
+    if not volume_geometry.has_isotropic_voxels():
+        return False
+    if len(projection_geometry) != len(projections):
+        return False
+    det = (projection_geometry.detector
+           if isinstance(projection_geometry, ProjectionGeometrySequence)
+           else projection_geometry[0].detector)
+    return (int(np.asarray(det.rows).flat[0]), int(np.asarray(det.cols).flat[0])) \
+        == projections.shape[1:]
+
+
+def _streamed_bp(projections: np.ndarray, projection_geometry,
+                 volume_geometry: VolumeGeometry, filter: Any,
+                 kernel: VoxelDrivenConeBP = None):
+    """Backprojection (with FDK pre-weighting and filtering when ``filter``
+    is given) in 32-angle chunks through a two-slot ring of 32-layer
+    textures, so no whole-scan texture is allocated. Host projections are
+    streamed: while the host stages chunk c+1 into pinned memory and a
+    copy stream uploads it, the GPU pre-weights and filters chunk c,
+    copies it into a texture and backprojects it onto the volume; the
+    caller's array is left untouched (the reference also processes a
+    device copy). Device projections are pre-weighted and filtered in
+    place, as in the reference, then backprojected chunk by chunk. Every
+    kernel is the one of the whole-scan path, on the same angles and in the
+    same summation order, so the volume is bit for bit the same."""
+    from . import processing
+
+    t = _arrays.torch()
+    L = _native.load()
+    n, rows, cols = projections.shape
+    st = _stream_buffers(rows, cols)
+    cs = t.cuda.current_stream()
+    stream = _native.current_stream()
+    K = kernel if kernel is not None else VoxelDrivenConeBP()
+    K.compile()
+    K.set_params(K.geoms2params(projection_geometry, volume_geometry))
+    vol = t.empty(tuple(int(s) for s in volume_geometry.shape),
+                  dtype=t.float32, device="cuda")
+    vdesc = _native.volume_desc(vol, K._vol_axs)
+    vox_vol = float(np.float32(volume_geometry.voxel_volume()))
+    params = K._params_dev.data_ptr()
+    if filter is not None:
+        pw = t.from_numpy(processing.preweight_params(
+            projection_geometry)).cuda()
+        P = processing.padded_length(cols)
+        h = processing._device_filter(P, filter)
+    if st.get("last") is not None:
+        # the ring's previous user may run on another stream
+        cs.wait_event(st["last"])
+        st["copy"].wait_event(st["last"])
+    on_host = isinstance(projections, np.ndarray)
+    if on_host:
+        src = t.from_numpy(projections)
+    else:
+        src = _arrays.as_tensor(projections)
+        if filter is not None:
+            whole = _native.projections_desc(src)
+            _native.check(L.kk_preweight(whole, pw.data_ptr(), stream))
+            _native.check(L.kk_filter_rows(whole, h.data_ptr(), P, stream))
+    staged, used = [None, None], [None, None]
+    for c, a in enumerate(range(0, n, _CHUNK)):
+        m, b = min(_CHUNK, n - a), c & 1
+        texs = st["tex"].get(m)
+        if texs is None:
+            texs = [_native.Layered(m, rows, cols, _native.KK_F32)
+                    for _ in range(2)]
+            st["tex"][m] = texs
+        if not on_host:
+            texs[b].copy_from(src[a:a + m])
+            _native.check(L.kk_cone_bp_layered(
+                texs[b].handle, vdesc, params + a * 12 * 4, vox_vol,
+                int(c > 0), 0, stream))
+            continue
+        if staged[b] is not None:
+            staged[b].synchronize()  # the upload from this block is done
+        host = st["host"][b][:m]
+        host.copy_(src[a:a + m])
+        dev = st["dev"][b][:m]
+        with t.cuda.stream(st["copy"]):
+            if used[b] is not None:
+                st["copy"].wait_event(used[b])
+            dev.copy_(host, non_blocking=True)
+            staged[b] = t.cuda.Event()
+            staged[b].record(st["copy"])
+        cs.wait_event(staged[b])
+        pdesc = _native.projections_desc(dev)
+        if filter is not None:
+            _native.check(L.kk_preweight(pdesc, pw.data_ptr() + a * 13 * 8,
+                                         stream))
+            _native.check(L.kk_filter_rows(pdesc, h.data_ptr(), P, stream))
+        texs[b].copy_from(dev)
+        used[b] = t.cuda.Event()
+        used[b].record(cs)
+        _native.check(L.kk_cone_bp_layered(
+            texs[b].handle, vdesc, params + a * 12 * 4, vox_vol,
+            int(c > 0), 0, stream))
+    st["last"] = t.cuda.Event()
+    st["last"].record(cs)
+    return vol
+
+
 def bp(projections: Any, projection_geometry, volume_geometry: VolumeGeometry,
        filter: Any = None, preproc_fn: Callable = None,
        kernel: BaseKernel = None, out=None,
        projection_axes: Sequence[int] = (0, 1, 2), **kwargs):
     """X-ray backprojection, optionally with FDK pre-weighting and
     filtering (``algo.py:52-126``). Device float32 projections are
-    pre-processed in place, as in the reference. Returns a host array (or
-    fills a host ``out``)."""
+    pre-processed in place, as in the reference. Host (NumPy) projections
+    are streamed to the GPU in 32-angle chunks that overlap the upload
+    with the pre-processing and backprojection of the previous chunk.
+    Returns a host array (or fills a host ``out``)."""
     t = _arrays.torch()
+    if _can_stream(projections, projection_geometry, volume_geometry,
+                   preproc_fn, kernel, out, projection_axes, kwargs):
+        vol = _streamed_bp(projections, projection_geometry, volume_geometry,
+                           filter, kernel)
+        if isinstance(out, np.ndarray):
+            out[...] = vol.cpu().numpy()
+            return out
+        return _host_copy(vol)
     if out is not None and _arrays.is_device_array(out):
         out_gpu = _arrays.as_tensor(out, dtype=t.float32)
     else:

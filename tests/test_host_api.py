@@ -162,3 +162,39 @@ def test_autotuner_reuses_its_json_cache(tmp_path):
     assert tuner.pick("fp_axis_group:[[8,8,8],6,[9,9]]", (1, 2, 4),
                       calls.append) == 2
     assert calls == []
+
+
+def test_streamed_bp_is_taken_only_for_host_projections_in_default_layout():
+    """``kernelkit.algo._can_stream``: NumPy projections in the default
+    layout with the default backprojector take the chunked path; other
+    layouts, pre-processing callbacks and other kernels take the general
+    one (device arrays are checked on the GPU)."""
+    import torch
+
+    from kernelkit import algo
+    from kernelkit.kernels import VoxelDrivenConeBP
+
+    det = kk.Detector(rows=4, cols=6, pixel_height=1.0, pixel_width=1.0)
+    g0 = kk.ProjectionGeometry([-10.0, 0, 0], [10.0, 0, 0], det)
+    pgs = [kk.rotate(g0, yaw=0.1 * k) for k in range(3)]
+    vg = kk.resolve_volume_geometry(shape=(4, 4, 4), voxel_size=1.0)
+    y = np.zeros((3, 4, 6), np.float32)
+    ok = dict(preproc_fn=None, kernel=None, out=None,
+              projection_axes=(0, 1, 2), kwargs={})
+    assert algo._can_stream(y, pgs, vg, **ok)
+    assert algo._can_stream(y, pgs, vg, **{**ok, "kernel": VoxelDrivenConeBP()})
+    assert algo._can_stream(y, pgs, vg, **{**ok, "out": np.zeros((4, 4, 4))})
+    assert not algo._can_stream(torch.from_numpy(y), pgs, vg, **ok)  # host tensor
+    assert not algo._can_stream(y.tolist(), pgs, vg, **ok)
+    assert not algo._can_stream(y[::-1], pgs, vg, **ok)      # negative stride
+    assert not algo._can_stream(y.astype(">f4"), pgs, vg, **ok)
+    assert not algo._can_stream(y.astype(np.int16), pgs, vg, **ok)
+    assert algo._can_stream(y.astype(np.float64), pgs, vg, **ok)
+    assert not algo._can_stream(y, pgs, vg, **{**ok, "preproc_fn": print})
+    assert not algo._can_stream(y, pgs, vg,
+                                **{**ok, "projection_axes": (1, 0, 2)})
+    assert not algo._can_stream(
+        y, pgs, vg, **{**ok, "kernel": VoxelDrivenConeBP(interpolation="exact")})
+    assert not algo._can_stream(y[:2], pgs, vg, **ok)        # count mismatch
+    assert not algo._can_stream(y[:, :3], pgs, vg, **ok)     # detector mismatch
+    assert not algo._can_stream(y, pgs, vg, **{**ok, "kwargs": {"x": 1}})
