@@ -65,9 +65,9 @@ __device__ __forceinline__ void bp_block(const BpArgs& L, int bx, int by, int bz
         vacc[i] = 0.f;
         if (active && i < cnt) {
             if (L.load_mode == LOAD_VOL)
-                vacc[i] = ld_rw(vol + vbase + i * vstep);
+                vacc[i] = ld_cs(vol + vbase + i * vstep);
             else if (L.load_mode == LOAD_WORK)
-                vacc[i] = L.work[wbase + i * wstep];
+                vacc[i] = ld_cs(L.work + wbase + i * wstep);
         }
     }
 
@@ -118,17 +118,17 @@ __device__ __forceinline__ void bp_block(const BpArgs& L, int bx, int by, int bz
         if (i >= cnt) break;
         TV* p = vol + vbase + i * vstep;
         if (L.store_mode == STORE_WORK) {
-            L.work[wbase + i * wstep] = vacc[i];
+            st_cs(L.work + wbase + i * wstep, vacc[i]);
         } else if (EPI == BP_UPDATE) {
             const int64_t e = vbase + i * vstep;
-            float x = ld_rw(p);
+            float x = ld_cs(p);
             x = __fsub_rn(x, __fmul_rn(vacc[i], ld((const TV*)L.upd_scale + e)));
             if (L.upd_mask) x = __fmul_rn(x, ld((const TV*)L.upd_mask + e));
             if (L.has_min) x = fmaxf(x, L.vmin);
             if (L.has_max) x = fminf(x, L.vmax);
-            st(p, x);
+            st_cs(p, x);
         } else {
-            st(p, vacc[i]);
+            st_cs(p, vacc[i]);
         }
     }
 }

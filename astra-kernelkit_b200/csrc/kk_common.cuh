@@ -48,6 +48,18 @@ __device__ __forceinline__ void st<__nv_bfloat16>(__nv_bfloat16* p, float v) {
 template <>
 __device__ __forceinline__ void st<__half>(__half* p, float v) { *p = __float2half_rn(v); }
 
+// Streaming (evict-first) load and store for data touched once per launch,
+// such as the volume a backprojection chunk reads and rewrites: it then
+// does not push the chunk's projections out of L2. Same values as ld_rw/st.
+template <typename T>
+__device__ __forceinline__ float ld_cs(const T* p) { return ld_rw(p); }
+template <>
+__device__ __forceinline__ float ld_cs<float>(const float* p) { return __ldcs(p); }
+template <typename T>
+__device__ __forceinline__ void st_cs(T* p, float v) { st(p, v); }
+template <>
+__device__ __forceinline__ void st_cs<float>(float* p, float v) { __stcs(p, v); }
+
 // ---------------------------------------------------------------------------
 // paired float32 arithmetic (sm_100 FADD2/FMUL2/FFMA2): one instruction
 // performs the same IEEE operation on two independent lanes, bit for bit
