@@ -133,9 +133,32 @@ __device__ __forceinline__ void bp_block(const BpArgs& L, int bx, int by, int bz
     }
 }
 
+// Blocks run in super-columns: TZ x TY blocks of the two faster axes (up
+// to 256 x 512 voxels) swept along the slowest axis, so the blocks in
+// flight at any time cover a compact region of the volume whose footprint
+// on each projection is small, and the chunk's projections are re-read
+// from L2 rather than DRAM (headline BP 97.7 -> 92.6 ms against the plain
+// x-fastest order, whose in-flight slab covers most of every projection).
+// TZ, TY are the largest powers of two up to 8 and 64 dividing the grid's
+// extents, so the map below is a bijection of the grid.
+__device__ __forceinline__ void bp_tile_order(int& bx, int& by, int& bz) {
+    const int nx = gridDim.x, ny = gridDim.y, nz = gridDim.z;
+    const int TZ = min(8, nx & -nx), TY = min(64, ny & -ny);
+    const int lin = blockIdx.x + nx * (blockIdx.y + ny * blockIdx.z);
+    const int per_x = TZ * TY, col_blocks = per_x * nz;
+    const int col = lin / col_blocks, r = lin - col * col_blocks;
+    bz = r / per_x;
+    const int q = r - bz * per_x;
+    const int scx = nx / TZ;
+    bx = (col % scx) * TZ + q % TZ;
+    by = (col / scx) * TY + q / TZ;
+}
+
 template <typename TP, typename TV, bool TEX8, int EPI, int FETCH>
 __global__ void __launch_bounds__(BP_TILE_2* BP_TILE_1) cone_bp_kernel(const BpArgs L) {
-    bp_block<TP, TV, TEX8, EPI, FETCH>(L, blockIdx.x, blockIdx.y, blockIdx.z);
+    int bx, by, bz;
+    bp_tile_order(bx, by, bz);
+    bp_block<TP, TV, TEX8, EPI, FETCH>(L, bx, by, bz);
 }
 
 // Many problems in one launch (one 32-angle chunk of each): argument
