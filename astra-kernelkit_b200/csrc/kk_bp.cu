@@ -140,11 +140,10 @@ __device__ __forceinline__ void bp_block(const BpArgs& L, int bx, int by, int bz
 // from L2 rather than DRAM (headline BP 97.7 -> 92.6 ms against the plain
 // x-fastest order, whose in-flight slab covers most of every projection).
 // TZ, TY are the largest powers of two up to 8 and 64 dividing the grid's
-// extents, so the map below is a bijection of the grid.
-__device__ __forceinline__ void bp_tile_order(int& bx, int& by, int& bz) {
-    const int nx = gridDim.x, ny = gridDim.y, nz = gridDim.z;
+// extents nx, ny, so the map from the linear block index is a bijection of
+// the nx x ny x nz grid.
+__device__ __forceinline__ void bp_tile_order(int lin, int nx, int ny, int nz, int& bx, int& by, int& bz) {
     const int TZ = min(8, nx & -nx), TY = min(64, ny & -ny);
-    const int lin = blockIdx.x + nx * (blockIdx.y + ny * blockIdx.z);
     const int per_x = TZ * TY, col_blocks = per_x * nz;
     const int col = lin / col_blocks, r = lin - col * col_blocks;
     bz = r / per_x;
@@ -157,7 +156,8 @@ __device__ __forceinline__ void bp_tile_order(int& bx, int& by, int& bz) {
 template <typename TP, typename TV, bool TEX8, int EPI, int FETCH>
 __global__ void __launch_bounds__(BP_TILE_2* BP_TILE_1) cone_bp_kernel(const BpArgs L) {
     int bx, by, bz;
-    bp_tile_order(bx, by, bz);
+    bp_tile_order(blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z), gridDim.x, gridDim.y,
+                  gridDim.z, bx, by, bz);
     bp_block<TP, TV, TEX8, EPI, FETCH>(L, bx, by, bz);
 }
 
@@ -184,7 +184,10 @@ __global__ void __launch_bounds__(BP_TILE_2* BP_TILE_1) cone_bp_batched_kernel(c
     __syncthreads();
     const int t = b - B.block_start[i];
     const int tx = B.tiles[i][0], ty = B.tiles[i][1];
-    bp_block<float, float, true, EPI, FETCH_TEX>(Ls, t % tx, (t / tx) % ty, t / (tx * ty));
+    const int tz = (B.block_start[i + 1] - B.block_start[i]) / (tx * ty);
+    int bx, by, bz;
+    bp_tile_order(t, tx, ty, tz, bx, by, bz);
+    bp_block<float, float, true, EPI, FETCH_TEX>(Ls, bx, by, bz);
 }
 
 }  // namespace kk
