@@ -51,6 +51,11 @@ struct FpArgs {
     int rank[3];  // memory rank of each world axis: 0 fastest .. 2 slowest
     cudaTextureObject_t vtex;  // layered texture of the volume, or 0
     int off32;    // every element offset of the volume fits in 31 bits
+    // slices [s_begin, s_end) of every ray's own slice axis are traced in
+    // this launch (a multiple of the slab); the epilogue (residual, storage
+    // rounding) only in the launch whose final_pass is set
+    int s_begin, s_end;
+    int final_pass;
 };
 
 struct BpArgs {

@@ -87,7 +87,8 @@ EXPORTS = ("kk_cone_fp", "kk_cone_fp_residual", "kk_cone_fp_layered",
            "kk_cone_bp_update", "kk_layered_create", "kk_layered_copy",
            "kk_layered_destroy", "kk_cone_bp_layered",
            "kk_cone_bp_layered_update", "kk_preweight", "kk_filter_rows",
-           "kk_reciprocal", "kk_sirt_update", "kk_last_error",
+           "kk_reciprocal", "kk_sirt_update", "kk_fp_set_span",
+           "kk_fp_launches", "kk_last_error",
            "kk_abi_version")
 
 _lib = None
@@ -136,6 +137,8 @@ def load():
     L.kk_filter_rows.argtypes = [P(kk_projections), vp, i64, vp]
     L.kk_reciprocal.argtypes = [vp, i64, vp]
     L.kk_sirt_update.argtypes = [vp, vp, vp, vp, f32, f32, i32, i32, i64, vp]
+    L.kk_fp_set_span.argtypes = [i32]
+    L.kk_fp_launches.argtypes = [i32, i32, i32]
     for name in EXPORTS[:-2]:
         getattr(L, name).restype = ctypes.c_int
     L.kk_last_error.restype = ctypes.c_char_p

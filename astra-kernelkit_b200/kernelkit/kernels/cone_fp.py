@@ -475,4 +475,22 @@ class RayDrivenConeFP(BaseKernel):
             self._interp, self.slices_per_block, _native.current_stream()))
 
 
-__all__ = ["RayDrivenConeFP", "ConeFPParams"]
+def set_slices_per_launch(slices: int = 0) -> None:
+    """How many slices of every ray's own slice axis one forward-projection
+    launch traces (float32 projections): 0 = the default (256), -1 = the
+    whole ray in one launch. Results are the same bit for bit; shorter
+    spans keep the volume band each launch reads in L2. Process-wide."""
+    _native.check(_native.load().kk_fp_set_span(int(slices)))
+
+
+def launches_per_projection(max_slices: int, slab: int = 16,
+                            float32: bool = True) -> int:
+    """Kernel launches of one forward projection of a volume whose longest
+    axis has ``max_slices`` voxels."""
+    return int(_native.load().kk_fp_launches(
+        int(max_slices), int(slab),
+        _native.KK_F32 if float32 else _native.KK_F16))
+
+
+__all__ = ["RayDrivenConeFP", "ConeFPParams", "set_slices_per_launch",
+           "launches_per_projection"]

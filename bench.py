@@ -292,8 +292,10 @@ def load_peaks():
 
 
 def load_traffic(workload, kernel):
-    """DRAM bytes per launch of ``kernel`` from the committed ncu summary
-    (profiles/traffic.json), scaled to ``workload``; None if absent."""
+    """DRAM bytes of ``kernel`` from the committed ncu summary
+    (profiles/traffic.json: per forward projection, i.e. summed over its
+    slice-span launches, for the FP; per 32-angle launch for the BP) at
+    ``workload``; None if absent."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             t = json.load(f)
@@ -739,6 +741,8 @@ def run_ours(args):
         del dev_in, dev_y, dev_out
 
     peak, peak_kind = load_peaks()
+    from kernelkit.kernels.cone_fp import launches_per_projection
+    fp_launches = launches_per_projection(max(shape))
     fp_bytes = 4.0 * nupd  # algorithmic: one float32 voxel operand / update
     roofline = {"kernel": "cone_fp_kernel", "bound": "hbm",
                 "achieved": fp_bytes / (t_fp * 1e-3) / 1e9, "peak": peak,
@@ -746,7 +750,10 @@ def run_ours(args):
                 "frac": fp_bytes / (t_fp * 1e-3) / 1e9 / peak,
                 "peak_kind": peak_kind,
                 "traffic": load_traffic(args.workload, "cone_fp_kernel"),
-                "algorithmic_bytes_per_launch": fp_bytes}
+                "algorithmic_bytes_per_launch": fp_bytes,
+                # one forward projection is fp_launches launches of slice
+                # spans: bytes, time and traffic are per projection
+                "per": f"forward projection ({fp_launches} launches)"}
     # The backprojector samples one bilinear texel quad per update; its
     # ceiling is the texture unit's fetch rate, measured on this GPU model
     # with astra-kernelkit_b200/csrc/probes/tex_rate.cu (3.83 float32
@@ -766,7 +773,7 @@ def run_ours(args):
     kernels = {
         # "traffic": ncu DRAM bytes per launch (profiles/), "ms": all
         # launches of one operator application
-        "cone_fp_kernel": {"ms": t_fp, "launches": 1,
+        "cone_fp_kernel": {"ms": t_fp, "launches": fp_launches,
                            "gups": nupd / (t_fp * 1e-3) / 1e9,
                            "achieved_gbs": fp_bytes / (t_fp * 1e-3) / 1e9,
                            "traffic": load_traffic(args.workload,
@@ -820,7 +827,7 @@ def run_ours(args):
             "texture_roofline": texture_roofline, "cpu_baseline": cpu,
             "kernels": kernels,
             # per step: one FP launch and one BP launch per 32-angle chunk
-            "gpu_launches": args.steps * (1 + (len(pgs) + 31) // 32),
+            "gpu_launches": args.steps * (fp_launches + (len(pgs) + 31) // 32),
             "clocks": clocks, "sirt": sirt, "batched": batched,
         }
         print(json.dumps(line), flush=True)

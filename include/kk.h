@@ -154,6 +154,20 @@ KK_API int kk_cone_fp_layered(const kk_layered* vtex, const kk_volume* vol,
                               const kk_fp_residual* residual, int32_t slab,
                               int32_t additive, void* stream);
 
+/* Launch split of the three entry points above (no counterpart in the
+ * reference, whose FP is one launch): with float32 projections a
+ * projection is traced in launches of `slices` slices of every ray's own
+ * slice axis (a multiple of the slab; the running float32 sums are carried
+ * in the projections, so the result is bit for bit that of one launch)
+ * and each launch reads a band of the volume that stays in L2. slices = 0
+ * restores the default (256), -1 selects one launch. Process-wide. */
+KK_API int kk_fp_set_span(int32_t slices);
+
+/* Number of kernel launches kk_cone_fp* makes for a volume whose longest
+ * axis has max_slices voxels, with this slab and projection dtype. */
+KK_API int32_t kk_fp_launches(int32_t max_slices, int32_t slab,
+                              int32_t proj_dtype);
+
 /* Exact adjoint (transpose) of kk_cone_fp for the same records,
  * out_scale, interp and slab: vol = A^T proj (additive=0) or vol += A^T
  * proj, bit for bit the weights kk_cone_fp applies (same ray set-up, same

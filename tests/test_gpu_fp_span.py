@@ -1,0 +1,52 @@
+"""Forward projection traced in several launches of slice spans
+(``kk_fp_set_span``): the running float32 sums are carried in the
+projections between launches, so every span gives the one-launch result
+bit for bit, with the plain store, the additive form and the SIRT
+residual epilogue."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+import kernelkit as kk
+from helpers import build_case, case_volume
+from kernelkit.kernels import RayDrivenConeFP
+from kernelkit.kernels.cone_fp import set_slices_per_launch
+
+pytestmark = pytest.mark.gpu
+
+
+def _fp(pgs, vg, vol, mode):
+    K = RayDrivenConeFP()
+    K.compile()
+    K.set_params(K.geoms2params(pgs, vg))
+    det = pgs[0].detector
+    out = torch.full((len(pgs), det.rows, det.cols), 0.25, device="cuda")
+    if mode == "store":
+        K(vol, pgs, vg, out, additive=False)
+    elif mode == "additive":
+        K(vol, pgs, vg, out, additive=True)
+    else:
+        g = torch.Generator(device="cuda").manual_seed(5)
+        y = torch.rand(out.shape, generator=g, device="cuda")
+        w = torch.rand(out.shape, generator=g, device="cuda")
+        K.residual(vol, pgs, vg, out, y, w)
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+@pytest.mark.parametrize("case", ["small", "alldirs", "config1"])
+@pytest.mark.parametrize("mode", ["store", "additive", "residual"])
+def test_slice_spans_give_the_one_launch_result(case, mode):
+    pgs, vg = build_case(case)
+    vol = torch.from_numpy(case_volume(case, vg)).float().cuda()
+    try:
+        set_slices_per_launch(-1)
+        ref = _fp(pgs, vg, vol, mode)
+        for span in (16, 48, 100, 0):
+            set_slices_per_launch(span)
+            assert np.array_equal(_fp(pgs, vg, vol, mode), ref), span
+    finally:
+        set_slices_per_launch(0)
+    assert np.abs(ref).max() > 0

@@ -84,3 +84,25 @@ def test_interpolation_mode_checked():
     rc = L.kk_cone_fp(vol, proj, ctypes.c_void_p(0x3000), osc, 9, 16, 0, None)
     assert rc == _native.KK_ERR_INVALID_ARGUMENT
     assert b"interpolation" in L.kk_last_error()
+
+
+def test_fp_launch_split_is_host_logic():
+    """kk_fp_launches / kk_fp_set_span (no GPU needed): float32 projections
+    of volumes longer than 256 slices are traced in 256-slice launches by
+    default; 16-bit projections always in one launch."""
+    from kernelkit.kernels.cone_fp import (launches_per_projection,
+                                           set_slices_per_launch)
+
+    assert launches_per_projection(256) == 1
+    assert launches_per_projection(512) == 2
+    assert launches_per_projection(1024) == 4
+    assert launches_per_projection(1024, float32=False) == 1
+    try:
+        set_slices_per_launch(-1)
+        assert launches_per_projection(1024) == 1
+        set_slices_per_launch(100)  # rounded up to 112 = 7 slabs of 16
+        assert launches_per_projection(512) == 5
+        with pytest.raises(Exception):
+            set_slices_per_launch(-2)
+    finally:
+        set_slices_per_launch(0)
