@@ -87,6 +87,14 @@ def _stream_buffers(rows: int, cols: int) -> dict:
     return st
 
 
+def release_stream_buffers() -> None:
+    """Free the staging, device and texture ring that ``bp``/``fdk`` keep
+    between calls for the last detector shape (waits for its last use)."""
+    st = _STREAM.pop(next(iter(_STREAM)), None) if _STREAM else None
+    if st is not None and st.get("last") is not None:
+        st["last"].synchronize()
+
+
 def _can_stream(projections, projection_geometry, volume_geometry, preproc_fn,
                 kernel, out, projection_axes, kwargs) -> bool:
     """The chunked path takes host (NumPy) projections, or a C-contiguous
@@ -455,4 +463,4 @@ def sirt(projections: np.ndarray, projection_geometry: Any,
     return _host_copy(x)
 
 
-__all__ = ["fp", "bp", "fbp", "fdk", "sirt", "SIRT"]
+__all__ = ["fp", "bp", "fbp", "fdk", "sirt", "SIRT", "release_stream_buffers"]

@@ -73,6 +73,15 @@ def test_streamed_fdk_out_argument_and_reuse():
     assert np.array_equal(kk.fdk(y, pgs, vg), ref)
 
 
+def test_release_and_rebuild_the_ring():
+    pgs, vg = _scan(40)
+    y = _projections(pgs, 4)
+    ref = kk.fdk(y, pgs, vg)
+    algo.release_stream_buffers()
+    assert not algo._STREAM
+    assert np.array_equal(kk.fdk(y, pgs, vg), ref)
+
+
 def test_streamed_on_a_side_stream():
     pgs, vg = _scan(70)
     y = _projections(pgs, 3)
