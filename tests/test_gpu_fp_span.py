@@ -50,3 +50,26 @@ def test_slice_spans_give_the_one_launch_result(case, mode):
     finally:
         set_slices_per_launch(0)
     assert np.abs(ref).max() > 0
+
+
+def test_slice_spans_with_a_list_of_projection_arrays():
+    """Per-angle output arrays (the pointer-table form) carry the running
+    sums between span launches like one strided array."""
+    pgs, vg = build_case("alldirs")
+    vol = torch.from_numpy(case_volume("alldirs", vg)).float().cuda()
+    K = RayDrivenConeFP()
+    K.compile()
+    K.set_params(K.geoms2params(pgs, vg))
+    det = pgs[0].detector
+    try:
+        outs = []
+        for span in (-1, 16):
+            set_slices_per_launch(span)
+            lst = [torch.full((det.rows, det.cols), 0.5, device="cuda")
+                   for _ in pgs]
+            K(vol, pgs, vg, lst, additive=True)
+            torch.cuda.synchronize()
+            outs.append(torch.stack(lst).cpu().numpy())
+    finally:
+        set_slices_per_launch(0)
+    assert np.array_equal(outs[0], outs[1])
