@@ -126,7 +126,7 @@ def _can_stream(projections, projection_geometry, volume_geometry, preproc_fn,
         return False
     if not volume_geometry.has_isotropic_voxels():
         return False
-    if len(projection_geometry) != len(projections):
+    if len(projections) == 0 or len(projection_geometry) != len(projections):
         return False
     det = (projection_geometry.detector
            if isinstance(projection_geometry, ProjectionGeometrySequence)

@@ -196,5 +196,6 @@ def test_streamed_bp_is_taken_only_for_host_projections_in_default_layout():
     assert not algo._can_stream(
         y, pgs, vg, **{**ok, "kernel": VoxelDrivenConeBP(interpolation="exact")})
     assert not algo._can_stream(y[:2], pgs, vg, **ok)        # count mismatch
+    assert not algo._can_stream(y[:0], pgs[:0], vg, **ok)    # no angles
     assert not algo._can_stream(y[:, :3], pgs, vg, **ok)     # detector mismatch
     assert not algo._can_stream(y, pgs, vg, **{**ok, "kwargs": {"x": 1}})
