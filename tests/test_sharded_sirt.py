@@ -106,7 +106,12 @@ class OracleShardOps:
         x.copy_(v)
 
 
-def _rank_main(rank, world, port, iters, lo, out):
+def _mask(shape):
+    """A seeded 0/1 mask (about 80 % ones)."""
+    return (np.random.default_rng(9).random(shape) < 0.8).astype(np.float64)
+
+
+def _rank_main(rank, world, port, iters, lo, masked, out):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port),
                       CUDA_VISIBLE_DEVICES="")
     import sys
@@ -126,15 +131,18 @@ def _rank_main(rank, world, port, iters, lo, out):
         y = A(vol)
         det = pgs[0].detector
         ops = OracleShardOps(A, AT, vol.shape, (b - a, det.rows, det.cols))
-        solver = ShardedSIRT(y, pgs[a:b], vg, ops=ops, min_constraint=lo)
+        mask = torch.from_numpy(_mask(vol.shape)) if masked else None
+        solver = ShardedSIRT(y, pgs[a:b], vg, ops=ops, min_constraint=lo,
+                             mask=mask)
         x = solver.run(iters).numpy().copy()
         out.put((rank, a, b, x))
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world,lo", [(2, None), (3, 0.0)])
-def test_sharded_sirt_equals_the_unsharded_oracle(world, lo):
+@pytest.mark.parametrize("world,lo,masked", [(2, None, False),
+                                             (3, 0.0, False), (2, 0.0, True)])
+def test_sharded_sirt_equals_the_unsharded_oracle(world, lo, masked):
     """ShardedSIRT over gloo ranks, each with a share of the angles, gives
     the oracle's SIRT over the whole scan."""
     iters = 3
@@ -142,7 +150,7 @@ def test_sharded_sirt_equals_the_unsharded_oracle(world, lo):
     q = ctx.Queue()
     port = _free_port()
     procs = [ctx.Process(target=_rank_main,
-                         args=(r, world, port, iters, lo, q))
+                         args=(r, world, port, iters, lo, masked, q))
              for r in range(world)]
     for p in procs:
         p.start()
@@ -157,7 +165,8 @@ def test_sharded_sirt_equals_the_unsharded_oracle(world, lo):
     # the shares tile the scan
     assert [r[1] for r in res][0] == 0 and res[-1][2] == len(pgs)
     A, AT = ops_for(pgs)
-    ref = oproc.sirt(A(vol), A, AT, vol.shape, iters, vmin=lo)
+    ref = oproc.sirt(A(vol), A, AT, vol.shape, iters, vmin=lo,
+                     mask=_mask(vol.shape) if masked else None)
     for _, _, _, x in res:
         np.testing.assert_allclose(x, ref, rtol=1e-9, atol=1e-12)
     assert np.linalg.norm(ref) > 0
