@@ -408,8 +408,11 @@ static void launch_fp_typed(const FpArgs& base, bool tex8, cudaStream_t s) {
     const int row_tiles = (L.rows + FP_ROWS_T - 1) / FP_ROWS_T;
     const int64_t blocks = (int64_t)row_tiles * L.n_angles * L.col_tiles;  // < 2^31: checked by the caller
     const int nmax = max(L.vn[0], max(L.vn[1], L.vn[2]));
-    // intermediate sums must stay float32: spans only for float32 output
-    const int span = std::is_same<TP, float>::value ? fp_span(nmax, L.slab) : 0;
+    // intermediate sums must stay float32: spans only for float32 output;
+    // and a residual computed in place (out is y or the weight) needs its
+    // operand intact until the last launch: one launch then
+    const bool in_place = EPI == FP_RESIDUAL && (L.res_y == L.out || L.res_w == L.out);
+    const int span = std::is_same<TP, float>::value && !in_place ? fp_span(nmax, L.slab) : 0;
     const int passes = span ? (nmax + span - 1) / span : 1;
     for (int p = 0; p < passes; ++p) {
         if (span) {

@@ -134,7 +134,9 @@ KK_API int kk_cone_fp(const kk_volume* vol, const kk_projections* proj,
                       int32_t interp, int32_t slab, int32_t additive,
                       void* stream);
 
-/* Forward projection with the SIRT residual epilogue (kk_fp_residual). */
+/* Forward projection with the SIRT residual epilogue (kk_fp_residual).
+ * out may be residual->y or residual->weight (computed in place; such a
+ * call runs as one launch, see kk_fp_set_span). */
 KK_API int kk_cone_fp_residual(const kk_volume* vol, const kk_projections* out,
                                const kk_fp_angle* angles,
                                const float* out_scale,
