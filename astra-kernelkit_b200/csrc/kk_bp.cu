@@ -516,10 +516,12 @@ static int bp_scratch_address(float** out) {
 
 extern "C" int kk_cone_bp_static(const kk_projections* proj, const kk_volume* vol, const kk_bp_angle* angles,
                                  float out_scale, int32_t interp, int32_t additive, void* stream) {
-    if (vol && vol->shape[0] > 0 && vol->shape[1] > 0 && vol->shape[2] > 0 &&
+    // only a 16-bit volume keeps its running sums in the buffer: a float32
+    // volume carries them itself, so its size is not limited
+    if (vol && vol->dtype != KK_F32 && vol->shape[0] > 0 && vol->shape[1] > 0 && vol->shape[2] > 0 &&
         vol->shape[0] * vol->shape[1] * vol->shape[2] > (int64_t)KK_STATIC_SCRATCH_VOXELS)
         return kk_fail(KK_ERR_INVALID_ARGUMENT,
-                       "kk_cone_bp_static: %lld voxels exceed the built-in buffer of %d voxels; "
+                       "kk_cone_bp_static: %lld 16-bit voxels exceed the built-in buffer of %d voxels; "
                        "use kk_cone_bp with a caller-provided work buffer",
                        (long long)(vol->shape[0] * vol->shape[1] * vol->shape[2]), KK_STATIC_SCRATCH_VOXELS);
     float* scratch = nullptr;

@@ -240,3 +240,5 @@ __device__ __forceinline__ float bilinear(const T* __restrict__ base, int64_t s1
 // ---------------------------------------------------------------------------
 int kk_fail(int status, const char* fmt, ...);
 int kk_check_launch(const char* what);
+int kk_allow_smem(const void* kernel, size_t bytes, const char* who);
+int kk_sm_count();

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <stdint.h>
 
 #include "kk_common.cuh"
@@ -153,12 +154,8 @@ extern "C" int kk_filter_rows(const kk_projections* proj, const double* h, int64
     // the row and the four interleaved copies of hx (2 cols + 8 taps)
     const int64_t hq = (2 * proj->cols + 8 + 3) / 4;
     const size_t smem = sizeof(double) * (size_t)(proj->cols + 4 * hq);
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(filter_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(sizeof(double) * (FILT_MAX_COLS + 4 * ((2 * FILT_MAX_COLS + 11) / 4))));
-        attr_set = true;
-    }
+    rc = kk_allow_smem((const void*)filter_rows_kernel, smem, "kk_filter_rows");
+    if (rc) return rc;
     const int threads = (int)std::min<int64_t>(FILT_BLOCK, ((proj->cols + 3) / 4 + 31) / 32 * 32);
     filter_rows_kernel<<<(unsigned)lines, threads, smem, (cudaStream_t)stream>>>(
         (float*)proj->data, proj->table, proj->stride[0], proj->stride[1], proj->stride[2], (int)proj->rows,
@@ -169,8 +166,7 @@ extern "C" int kk_filter_rows(const kk_projections* proj, const double* h, int64
 extern "C" int kk_reciprocal(float* data, int64_t n, void* stream) {
     if (!data || n < 0) return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_reciprocal: bad arguments");
     if (n == 0) return KK_OK;
-    int64_t blocks = (n + 255) / 256;
-    if (blocks > 148 * 32) blocks = 148 * 32;
+    const int64_t blocks = std::min<int64_t>((n + 255) / 256, (int64_t)kk_sm_count() * 16);
     reciprocal_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(data, n);
     return kk_check_launch("kk_reciprocal");
 }
@@ -179,8 +175,7 @@ extern "C" int kk_sirt_update(float* x, const float* g, const float* scale, cons
                               float max_value, int32_t has_min, int32_t has_max, int64_t n, void* stream) {
     if (!x || !g || !scale || n < 0) return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_sirt_update: bad arguments");
     if (n == 0) return KK_OK;
-    int64_t blocks = (n + 255) / 256;
-    if (blocks > 148 * 32) blocks = 148 * 32;
+    const int64_t blocks = std::min<int64_t>((n + 255) / 256, (int64_t)kk_sm_count() * 16);
     sirt_update_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(x, g, scale, mask, min_value, max_value,
                                                                          has_min, has_max, n);
     return kk_check_launch("kk_sirt_update");

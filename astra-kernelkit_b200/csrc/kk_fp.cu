@@ -494,6 +494,27 @@ static int fill_fp_args(FpArgs& L, const kk_volume* vol, const kk_projections* p
     return KK_OK;
 }
 
+// The residual epilogue reads y and weight at the element it writes, so
+// out may be y or weight itself (same base and layout: computed in place,
+// in one launch) but must not overlap either at an offset, where a thread
+// would read an element another thread has already overwritten.
+static int check_residual_aliasing(const kk_projections* out, const kk_fp_residual* res, const char* who) {
+    const size_t es = out->dtype == KK_F32 ? 4 : 2;
+    int64_t last = 0;
+    const int64_t n[3] = {out->n_angles, out->rows, out->cols};
+    for (int k = 0; k < 3; ++k) last += (n[k] - 1) * out->stride[k];
+    const uintptr_t lo = (uintptr_t)out->data, hi = lo + (uintptr_t)((last + 1) * (int64_t)es);
+    const void* ops[2] = {res->y, res->weight};
+    for (int i = 0; i < 2; ++i) {
+        const uintptr_t b = (uintptr_t)ops[i], e = b + (hi - lo);  // same layout as out
+        if (b == lo || e <= lo || b >= hi) continue;
+        return kk_fail(KK_ERR_INVALID_ARGUMENT,
+                       "%s: the output overlaps residual %s at an offset (in place is allowed only on the same "
+                       "elements)", who, i == 0 ? "y" : "weight");
+    }
+    return KK_OK;
+}
+
 extern "C" int kk_fp_set_span(int32_t slices) {
     if (slices < -1) return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_fp_set_span: %d slices", slices);
     g_fp_span = slices;
@@ -527,6 +548,8 @@ extern "C" int kk_cone_fp_residual(const kk_volume* vol, const kk_projections* o
         return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_cone_fp_residual: residual operands are NULL");
     if (out->table)
         return kk_fail(KK_ERR_UNSUPPORTED, "kk_cone_fp_residual: strided projections only");
+    rc = check_residual_aliasing(out, residual, "kk_cone_fp_residual");
+    if (rc) return rc;
 
     L.res_y = residual->y;
     L.res_w = residual->weight;
@@ -557,6 +580,8 @@ extern "C" int kk_cone_fp_layered(const kk_layered* vtex, const kk_volume* vol, 
         if (!residual->y || !residual->weight)
             return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: residual operands are NULL", who);
         if (proj->table) return kk_fail(KK_ERR_UNSUPPORTED, "%s: residual epilogue needs strided data", who);
+        rc = check_residual_aliasing(proj, residual, who);
+        if (rc) return rc;
         L.res_y = residual->y;
         L.res_w = residual->weight;
         return launch_fp<FP_RESIDUAL>(L, (int)proj->n_angles, vol->dtype, proj->dtype, true, (cudaStream_t)stream);

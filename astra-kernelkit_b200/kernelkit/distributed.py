@@ -71,6 +71,18 @@ class CudaShardOps:
         return t.zeros(tuple(int(s) for s in self.vg.shape),
                        dtype=t.float32, device="cuda")
 
+    def volume_array(self, a):
+        """``a`` (NumPy, torch, boolean or float) as a contiguous float32
+        device array of the volume's shape, as the reference converts the
+        SIRT mask (``algo.py:316-317``)."""
+        t = _arrays.torch()
+        v = _arrays.as_tensor(a, dtype=t.float32)
+        shape = tuple(int(s) for s in self.vg.shape)
+        if tuple(v.shape) != shape:
+            raise ValueError(f"array of shape {tuple(v.shape)} does not "
+                             f"match the volume {shape}")
+        return v.contiguous()
+
     def empty_projections(self):
         t = _arrays.torch()
         return t.zeros(self.shape, dtype=t.float32, device="cuda")
@@ -125,10 +137,22 @@ class ShardedSIRT:
 
         self.dist = dist
         self.group = group
+        # every rank needs a share of the angles; agree on that before any
+        # rank builds its operators, so that no rank fails alone while the
+        # others wait in a collective
+        t = _arrays.torch()
+        dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+        have = t.tensor([1 if len(projection_geometry) > 0 else 0],
+                        dtype=t.int32, device=dev)
+        dist.all_reduce(have, op=dist.ReduceOp.MIN, group=group)
+        if int(have.item()) == 0:
+            raise ValueError(
+                "ShardedSIRT needs at least one angle on every rank: the "
+                "scan has fewer angles than the process group has ranks")
         self.ops = ops or CudaShardOps(projection_geometry, volume_geometry)
         o = self.ops
         self.y = o.projections(projections)
-        self.mask = mask
+        self.mask = None if mask is None else o.volume_array(mask)
         self.lo, self.hi = min_constraint, max_constraint
         self.x = o.empty_volume()
         # R = 1 / A_k 1 (this rank's angles only)

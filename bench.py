@@ -37,7 +37,7 @@ import numpy as np  # noqa: E402
 
 METRIC = "cone FP+BP GUPS @512^3/720 ang"
 #: float32 2D-layered bilinear fetches per clock per SM of the B200's
-#: texture unit (astra-kernelkit_b200/csrc/probes/tex_rate.cu)
+#: texture unit, measured (profiles/texture_unit_rate.md)
 TMU_FETCH_PER_CLK_SM = 3.83
 UNIT = "GUPS"
 
@@ -609,6 +609,67 @@ def run_autograd_config3(steps=100, seed=1238):
             "cosine_to_backprojector_gradient": cos}
 
 
+def run_reference_kernels(w, pgs, vg, vol, proj, bp, reps=3):
+    """The reference's own CUDA kernels (its cone_fp.cu / cone_bp.cu
+    templates rendered with its default arguments and compiled for sm_100a
+    by oracle/build_ref.py) on this workload, after the timed region:
+    kernel-only time (CUDA events around its launch loops, inputs already
+    in its textures; median of ``reps`` after one warm-up), and, as the
+    checker, the rel. L2 between its outputs and ours on the same inputs:
+    FP of the same volume; BP of the reference's own sinogram by both."""
+    import torch
+
+    from kernelkit import _native
+    from kernelkit.kernels import RayDrivenConeFP, VoxelDrivenConeBP
+    from oracle import ref_kernels
+
+    if not ref_kernels.available():
+        return {"error": "oracle/_ref/libkkref.so not built"}
+    fpar = RayDrivenConeFP.geoms2params(pgs, vg)
+    rows12 = np.stack([np.asarray(p, np.float32) for p in fpar], axis=1)
+    osc = np.asarray(RayDrivenConeFP._output_scale(vg.voxel_size), np.float32)
+    bpar = VoxelDrivenConeBP.geoms2params(pgs, vg).reshape(-1, 12)
+    det = w["det"]
+    fp_ms, bp_ms = [], []
+    ref_fp = None
+    for k in range(reps + 1):
+        ref_fp, ms = ref_kernels.ref_cone_fp(vol, rows12, fpar.axes, det, det,
+                                             osc)
+        if k:
+            fp_ms.append(ms)
+    rel_fp = float((proj.double() - ref_fp.double()).norm()
+                   / ref_fp.double().norm())
+    ref_bp = None
+    for k in range(reps + 1):
+        ref_bp, ms = ref_kernels.ref_cone_bp(ref_fp, bpar, vg.shape,
+                                             float(vg.voxel_volume()))
+        if k:
+            bp_ms.append(ms)
+    tex = _native.Layered(len(pgs), det, det, _native.KK_F32)
+    tex.copy_from(ref_fp)
+    ours_bp = torch.empty_like(vol)
+    bp(tex, ours_bp, vg, additive=False)
+    torch.cuda.synchronize()
+    rel_bp = float((ours_bp.double() - ref_bp.double()).norm()
+                   / ref_bp.double().norm())
+    del tex, ref_fp, ref_bp, ours_bp
+    torch.cuda.empty_cache()
+    nupd = float(np.prod([int(s) for s in vg.shape])) * len(pgs)
+    t_fp, t_bp = statistics.median(fp_ms), statistics.median(bp_ms)
+    return {"fp_ms": t_fp, "bp_ms": t_bp,
+            "fp_gups": nupd / (t_fp * 1e-3) / 1e9,
+            "bp_gups": nupd / (t_bp * 1e-3) / 1e9,
+            "gups": 2 * nupd / ((t_fp + t_bp) * 1e-3) / 1e9,
+            "rel_l2_fp": rel_fp, "rel_l2_bp": rel_bp,
+            "source": "reference cone_fp.cu/cone_bp.cu templates rendered "
+                      "with the reference's defaults, built for sm_100a "
+                      "(oracle/build_ref.py); kernel-only CUDA events "
+                      f"around its launch loops, median of {reps} after one "
+                      "warm-up; rel_l2 = ours vs the reference on the same "
+                      "inputs (FP of the volume, BP of the reference's "
+                      "sinogram)"}
+
+
 def run_ours(args):
     import torch
 
@@ -756,9 +817,9 @@ def run_ours(args):
                 "per": f"forward projection ({fp_launches} launches)"}
     # The backprojector samples one bilinear texel quad per update; its
     # ceiling is the texture unit's fetch rate, measured on this GPU model
-    # with astra-kernelkit_b200/csrc/probes/tex_rate.cu (3.83 float32
-    # bilinear fetches per clock per SM), at the SM clock seen during the
-    # timed region.
+    # (3.83 float32 bilinear fetches per clock per SM,
+    # profiles/texture_unit_rate.md), at the SM clock seen during the timed
+    # region.
     sm_hz = 1e6 * float(clocks.get("sm_mhz") or clocks.get("sm_max_mhz")
                         or 1965.0)
     sms = torch.cuda.get_device_properties(0).multi_processor_count
@@ -769,7 +830,7 @@ def run_ours(args):
         "unit": "bilinear fetches/s",
         "frac": nupd / (t_bp * 1e-3) / tmu_peak,
         "peak_source": f"{TMU_FETCH_PER_CLK_SM} fetches/clk/SM measured "
-                       "(csrc/probes/tex_rate.cu) x SMs x SM clock"}
+                       "(profiles/texture_unit_rate.md) x SMs x SM clock"}
     kernels = {
         # "traffic": ncu DRAM bytes per launch (profiles/), "ms": all
         # launches of one operator application
@@ -784,6 +845,15 @@ def run_ours(args):
                            "traffic": load_traffic(args.workload,
                                                    "cone_bp_kernel")},
     }
+    refk = None
+    if rank == 0 and world == 1 and not args.no_reference_kernels:
+        try:
+            refk = run_reference_kernels(w, pgs, vg, vol, proj, bp)
+            if "gups" in refk:
+                refk["speedup"] = (2 * nupd / ((t_fp + t_bp) * 1e-3) / 1e9
+                                   / refk["gups"])
+        except Exception as e:  # noqa: BLE001
+            refk = {"error": f"{type(e).__name__}: {e}"[:300]}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = len(os.sched_getaffinity(0))
@@ -825,7 +895,7 @@ def run_ours(args):
                        "parallelism": f"replicas x{world}"},
             "e2e": e2e, "roofline": roofline,
             "texture_roofline": texture_roofline, "cpu_baseline": cpu,
-            "kernels": kernels,
+            "kernels": kernels, "reference_kernels": refk,
             # per step: one FP launch and one BP launch per 32-angle chunk
             "gpu_launches": args.steps * (fp_launches + (len(pgs) + 31) // 32),
             "clocks": clocks, "sirt": sirt, "batched": batched,
@@ -888,6 +958,8 @@ def main(argv=None):
                     default="headline")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-kernels", action="store_true",
+                    help="skip timing the reference's own CUDA kernels")
     ap.add_argument("--sirt-config5", action="store_true",
                     help="only run the 1024^3 SIRT storage comparison "
                          "(several minutes; prints its own JSON line)")

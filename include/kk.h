@@ -204,13 +204,17 @@ KK_API int kk_cone_bp(const kk_projections* proj, const kk_volume* vol,
 /* kk_cone_bp for callers that cannot allocate device memory (for example
  * an application whose device memory belongs to its own pooled allocator,
  * or a program that links this library but not the CUDA runtime): the
- * float32 running sums come from a buffer built into the library, of
- * 2^23 voxels (32 MiB, held on every GPU that loads the library until the
- * process exits). Larger volumes are rejected with KK_ERR_INVALID_ARGUMENT.
- * Nothing is allocated. The first call on a device looks up the buffer's
- * device address, so make it before capturing a stream. All calls share
- * the buffer: calls that may run at the same time on the GPU (different
- * streams) race and must not overlap. No counterpart in the reference. */
+ * float32 running sums of a 16-bit volume come from a buffer built into
+ * the library, of 2^23 voxels (32 MiB, held on every GPU that loads the
+ * library until the process exits). 16-bit volumes with more voxels are
+ * rejected with KK_ERR_INVALID_ARGUMENT; a float32 volume holds its own
+ * running sums and may have any size. Nothing is allocated. The first call
+ * on a device looks up the buffer's device address and keeps it, so make
+ * that call before capturing a stream, and do not call cudaDeviceReset on
+ * that device while the library is in use (the kept address would go
+ * stale). All calls share the buffer: calls that may run at the same time
+ * on the GPU (different streams) race and must not overlap. No
+ * counterpart in the reference. */
 KK_API int kk_cone_bp_static(const kk_projections* proj, const kk_volume* vol,
                              const kk_bp_angle* angles, float out_scale,
                              int32_t interp, int32_t additive, void* stream);

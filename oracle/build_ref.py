@@ -14,7 +14,8 @@ only the shared library lands in ``oracle/_ref/`` (git-ignored, shipped to
 the GPU machine with the rest of the tree). Without the reference checkout
 the recipe does nothing and a previously built library is used.
 
-Usage: ``python oracle/build_ref.py [--reference PATH]``
+Usage: ``python oracle/build_ref.py [--reference PATH]`` (default: the
+``KK_REFERENCE`` environment variable, else the checkout's usual place).
 """
 from __future__ import annotations
 
@@ -28,7 +29,8 @@ import tempfile
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_ref")
 OUT_LIB = os.path.join(OUT_DIR, "libkkref.so")
-DEFAULT_REFERENCE = "/root/reference"
+#: checkout of the reference (KK_REFERENCE overrides the default location)
+DEFAULT_REFERENCE = os.environ.get("KK_REFERENCE", "/root/reference")
 
 FP_KWARGS = dict(slices_per_block=16, rows_per_block=32, cols_per_block=32,
                  nr_projs_global=1024, volume_axes=(0, 1, 2),

@@ -4,7 +4,8 @@
 // rates that bound the cone-beam projectors' texture paths (the peak used
 // by bench.py's texture roofline).
 //
-// Build and run on the GPU:
+// Hardware characterisation, not part of the library. Build and run on
+// the GPU:
 //   nvcc -gencode arch=compute_100a,code=sm_100a -O3 -o tex_rate tex_rate.cu && ./tex_rate
 // All coordinates stay inside the 256^3 arrays (border addressing anyway).
 #include <cuda_runtime.h>

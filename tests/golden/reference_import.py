@@ -12,12 +12,14 @@ Euler-angle closed form (Shoemake, Graphics Gems IV).
 from __future__ import annotations
 
 import math
+import os
 import sys
 import types
 
 import numpy as np
 
-REFERENCE = "/root/reference"
+#: checkout of the reference (KK_REFERENCE overrides the default location)
+REFERENCE = os.environ.get("KK_REFERENCE", "/root/reference")
 
 
 def _cupy_stand_in():

@@ -73,3 +73,50 @@ def test_slice_spans_with_a_list_of_projection_arrays():
     finally:
         set_slices_per_launch(0)
     assert np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("target", ["y", "weight"])
+@pytest.mark.parametrize("span", [16, 0])
+def test_residual_in_place_matches_out_of_place(target, span):
+    """out may be the measured projections or the weight itself: the
+    residual is then computed in place, with any span setting, and equals
+    the out-of-place result bit for bit."""
+    pgs, vg = build_case("config1")
+    vol = torch.from_numpy(case_volume("config1", vg)).float().cuda()
+    K = RayDrivenConeFP()
+    K.compile()
+    K.set_params(K.geoms2params(pgs, vg))
+    det = pgs[0].detector
+    g = torch.Generator(device="cuda").manual_seed(9)
+    y = torch.rand((len(pgs), det.rows, det.cols), generator=g, device="cuda")
+    w = torch.rand(y.shape, generator=g, device="cuda")
+    try:
+        set_slices_per_launch(span)
+        ref = torch.empty_like(y)
+        K.residual(vol, pgs, vg, ref, y, w)
+        y2, w2 = y.clone(), w.clone()
+        out = y2 if target == "y" else w2
+        K.residual(vol, pgs, vg, out, y2, w2)
+        torch.cuda.synchronize()
+    finally:
+        set_slices_per_launch(0)
+    assert torch.equal(out, ref)
+
+
+def test_residual_partial_overlap_is_rejected():
+    """An output that overlaps y or the weight at an offset would read
+    elements other threads already overwrote: rejected, nothing launched."""
+    pgs, vg = build_case("small")
+    vol = torch.from_numpy(case_volume("small", vg)).float().cuda()
+    K = RayDrivenConeFP()
+    K.compile()
+    K.set_params(K.geoms2params(pgs, vg))
+    det = pgs[0].detector
+    n = len(pgs) * det.rows * det.cols
+    buf = torch.zeros(n + det.cols, device="cuda")
+    shape = (len(pgs), det.rows, det.cols)
+    y = buf[:n].view(shape)
+    out = buf[det.cols:].view(shape)
+    w = torch.ones(shape, device="cuda")
+    with pytest.raises(ValueError, match="overlaps"):
+        K.residual(vol, pgs, vg, out, y, w)

@@ -83,6 +83,9 @@ class OracleShardOps:
     def empty_projections(self):
         return torch.zeros(self.proj_shape, dtype=torch.float64)
 
+    def volume_array(self, a):
+        return torch.as_tensor(np.asarray(a, np.float64))
+
     def project(self, x, out):
         out.copy_(torch.from_numpy(self.A(x.numpy())))
 
@@ -170,6 +173,51 @@ def test_sharded_sirt_equals_the_unsharded_oracle(world, lo, masked):
     for _, _, _, x in res:
         np.testing.assert_allclose(x, ref, rtol=1e-9, atol=1e-12)
     assert np.linalg.norm(ref) > 0
+
+
+def _rank_empty_share(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port),
+                      CUDA_VISIBLE_DEVICES="")
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    for p in (root, os.path.join(root, "astra-kernelkit_b200"),
+              os.path.join(root, "tests")):
+        sys.path.insert(0, p)
+    import torch.distributed as dist
+    from kernelkit.distributed import ShardedSIRT, angle_shard
+
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        pgs, vg, vol, ops_for = _oracle_problem()
+        pgs = pgs[:world - 1]             # one angle short of a full share
+        a, b = angle_shard(len(pgs), world, rank)
+        try:
+            ShardedSIRT(None, pgs[a:b], vg, ops=object())
+            out.put((rank, "constructed"))
+        except ValueError as e:
+            out.put((rank, "ValueError" if "every rank" in str(e) else str(e)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_sirt_with_an_empty_share_fails_on_every_rank():
+    """Fewer angles than ranks: every rank raises the same ValueError
+    before any rank builds its operators, so none waits alone in a
+    collective."""
+    world = 3
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_empty_share, args=(r, world, port, q))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted((q.get(timeout=300) for _ in range(world)))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert [r[1] for r in res] == ["ValueError"] * world
 
 
 # ---- GPU ---------------------------------------------------------------
