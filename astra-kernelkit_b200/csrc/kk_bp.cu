@@ -350,11 +350,14 @@ extern "C" int kk_layered_create(int64_t layers, int64_t height, int64_t width, 
         return kk_fail(KK_ERR_UNSUPPORTED, "kk_layered_create: float32 or float16 texels only");
     cudaChannelFormatDesc ch = dtype == KK_F32 ? cudaCreateChannelDesc<float>() : cudaCreateChannelDescHalf();
     kk_layered* t = new kk_layered();
+    t->surf = 0;
+    t->tex = 0;
     t->layers = layers;
     t->height = height;
     t->width = width;
     t->dtype = dtype;
-    cudaError_t e = cudaMalloc3DArray(&t->array, &ch, make_cudaExtent(width, height, layers), cudaArrayLayered);
+    cudaError_t e = cudaMalloc3DArray(&t->array, &ch, make_cudaExtent(width, height, layers),
+                                      cudaArrayLayered | cudaArraySurfaceLoadStore);
     if (e != cudaSuccess) {
         delete t;
         return kk_fail(KK_ERR_CUDA, "kk_layered_create: %s", cudaGetErrorString(e));
@@ -368,7 +371,9 @@ extern "C" int kk_layered_create(int64_t layers, int64_t height, int64_t width, 
     td.readMode = cudaReadModeElementType;
     td.normalizedCoords = 0;
     e = cudaCreateTextureObject(&t->tex, &rd, &td, nullptr);
+    if (e == cudaSuccess) e = cudaCreateSurfaceObject(&t->surf, &rd);
     if (e != cudaSuccess) {
+        if (t->tex) cudaDestroyTextureObject(t->tex);
         cudaFreeArray(t->array);
         delete t;
         return kk_fail(KK_ERR_CUDA, "kk_layered_create: %s", cudaGetErrorString(e));
@@ -379,6 +384,7 @@ extern "C" int kk_layered_create(int64_t layers, int64_t height, int64_t width, 
 
 extern "C" int kk_layered_destroy(kk_layered* t) {
     if (!t) return KK_OK;
+    if (t->surf) cudaDestroySurfaceObject(t->surf);
     cudaDestroyTextureObject(t->tex);
     cudaFreeArray(t->array);
     delete t;

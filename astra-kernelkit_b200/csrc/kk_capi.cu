@@ -8,6 +8,7 @@
 #include <utility>
 
 #include "kk_common.cuh"
+#include "kk_async.cuh"
 
 static thread_local char g_last_error[512] = "";
 
@@ -63,4 +64,37 @@ int kk_sm_count() {
     if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
     seen[dev] = n;
     return n;
+}
+
+// cuTensorMapEncodeTiled, looked up once through the runtime's driver
+// entry point, so the library needs no link-time libcuda.
+typedef CUresult (*kk_encode_tiled_fn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                       const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                       CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int kk_encode_tile_map(CUtensorMap* map, CUtensorMapDataType type, int rank, void* base, const uint64_t* dims,
+                       const uint64_t* strides_bytes, const uint32_t* box, const char* who) {
+    static std::once_flag once;
+    static kk_encode_tiled_fn fn = nullptr;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (kk_encode_tiled_fn)p;
+    });
+    if (!fn) return kk_fail(KK_ERR_CUDA, "%s: cuTensorMapEncodeTiled is not available", who);
+    cuuint64_t d[5], s[4];
+    cuuint32_t b[5], e[5];
+    for (int k = 0; k < rank; ++k) {
+        d[k] = dims[k];
+        b[k] = box[k];
+        e[k] = 1;
+        if (k + 1 < rank) s[k] = strides_bytes[k];
+    }
+    const CUresult r = fn(map, type, (cuuint32_t)rank, base, d, s, b, e, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return kk_fail(KK_ERR_CUDA, "%s: cuTensorMapEncodeTiled failed (%d)", who, (int)r);
+    return KK_OK;
 }

@@ -92,6 +92,7 @@ enum BpFetch { FETCH_GLOBAL = 0, FETCH_TEX = 1 };
 struct kk_layered {
     cudaArray_t array;
     cudaTextureObject_t tex;
+    cudaSurfaceObject_t surf;  // float32 arrays: writable by kernels (FDK filter)
     int64_t layers, height, width;
     int32_t dtype;
 };

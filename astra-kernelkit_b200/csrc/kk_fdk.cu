@@ -7,7 +7,7 @@
 #include <mutex>
 #include <stdint.h>
 
-#include "kk_common.cuh"
+#include "kk_cone.cuh"
 
 namespace kk {
 
@@ -88,6 +88,159 @@ __global__ void __launch_bounds__(FILT_BLOCK)
 #pragma unroll
         for (int q = 0; q < 4; ++q)
             if (i0 + q < cols) base[(int64_t)(i0 + q) * sc] = __double2float_rn(acc[q]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// fused FDK pre-processing: pre-weighting, zero padding, FFT filtering and
+// the store into the backprojector's layered texture in one pass
+// ---------------------------------------------------------------------------
+// One block filters two detector rows at once: row a is the real part and
+// row b the imaginary part of one complex signal z of length P (rows
+// zero-padded from cols). The filter's response H is real and even, so
+// IFFT(H . FFT(z)) = (h * a) + i (h * b): the real and imaginary parts of
+// the filtered signal are the two filtered rows. The reference filters
+// each row with a float64 FFT in the same way (processing.py:111-126).
+//
+// The transform runs in shared memory in float64: decimation-in-frequency
+// radix-4 stages (and one radix-2 stage when log2 P is odd) leave the
+// spectrum in bit-reversed order, the multiplication by H reads H at the
+// bit-reversed index, and the inverse stages (conjugate twiddles, in
+// reverse order) take bit-reversed input back to natural order, so no
+// permutation pass is needed. W[k] = exp(-2 pi i k / P), k < P, comes from
+// the caller. Shared-memory index i is stored at i + i / 8 to spread the
+// strided accesses of the short stages over the banks.
+constexpr int FFT_THREADS = 256;
+constexpr int FFT_MAX_P = 8192;
+
+__device__ __forceinline__ int fpad(int i) { return i + (i >> 3); }
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 w) {
+    return make_double2(fma(a.x, w.x, -a.y * w.y), fma(a.x, w.y, a.y * w.x));
+}
+__device__ __forceinline__ double2 cmulc(double2 a, double2 w) {  // a * conj(w)
+    return make_double2(fma(a.x, w.x, a.y * w.y), fma(a.y, w.x, -a.x * w.y));
+}
+
+// The pre-weighted float32 value of one pixel, as kk_preweight stores it
+// (p *= |d - s| / |pixel - s| in float64, rounded once to float32).
+__device__ __forceinline__ double fdk_load(const float* row, int64_t sc, int c, int r, const double* g) {
+    const float p = row[(int64_t)c * sc];
+    if (!g) return (double)p;
+    double sq = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double q = __dadd_rn(__dadd_rn(g[k], __dmul_rn((double)c, g[3 + k])), __dmul_rn((double)r, g[6 + k]));
+        const double d = __dsub_rn(q, g[9 + k]);
+        sq = k == 0 ? __dmul_rn(d, d) : __dadd_rn(sq, __dmul_rn(d, d));
+    }
+    const double w = __ddiv_rn(g[12], __dsqrt_rn(sq));
+    return (double)__double2float_rn(__dmul_rn((double)p, w));
+}
+
+__global__ void __launch_bounds__(FFT_THREADS)
+    fdk_filter_kernel(const float* src, const uint64_t* src_table, int64_t sa, int64_t sr, int64_t sc, int n_lines,
+                      int rows, int cols, const double* __restrict__ geom, const double* __restrict__ H,
+                      const double2* __restrict__ W, int P, int log2P, float* dst, const uint64_t* dst_table,
+                      int64_t da, int64_t dr, int64_t dc, cudaSurfaceObject_t surf, int layer0) {
+    extern __shared__ double2 fz[];
+    const int tid = threadIdx.x;
+    const int line0 = 2 * blockIdx.x;
+    const bool two = line0 + 1 < n_lines;
+    const int a0 = line0 / rows, r0 = line0 % rows;
+    const int a1 = (line0 + 1) / rows, r1 = (line0 + 1) % rows;
+    const float* row0 = (src_table ? (const float*)src_table[a0] : src + (int64_t)a0 * sa) + (int64_t)r0 * sr;
+    const float* row1 = (src_table ? (const float*)src_table[a1] : src + (int64_t)a1 * sa) + (int64_t)r1 * sr;
+    const double* g0 = geom ? geom + 13 * (int64_t)a0 : nullptr;
+    const double* g1 = geom ? geom + 13 * (int64_t)a1 : nullptr;
+    for (int j = tid; j < P; j += FFT_THREADS) {
+        double re = 0.0, im = 0.0;
+        if (j < cols) {
+            re = fdk_load(row0, sc, j, r0, g0);
+            if (two) im = fdk_load(row1, sc, j, r1, g1);
+        }
+        fz[fpad(j)] = make_double2(re, im);
+    }
+    __syncthreads();
+    // forward: radix-4 decimation in frequency, then radix 2 if log2 P is odd
+    int len = P, lq = log2P - 2;  // lq = log2(len / 4)
+    for (; len >= 4; len >>= 2, lq -= 2) {
+        const int q = len >> 2, ts = P / len;
+        for (int t = tid; t < (P >> 2); t += FFT_THREADS) {
+            const int j = t & (q - 1), base = ((t >> lq) * len) + j;
+            const double2 a = fz[fpad(base)], b = fz[fpad(base + q)], c = fz[fpad(base + 2 * q)],
+                          d = fz[fpad(base + 3 * q)];
+            const double2 t0 = cadd(a, c), t1 = csub(a, c), t2 = cadd(b, d);
+            const double2 bd = csub(b, d);
+            const double2 t3 = make_double2(bd.y, -bd.x);  // (b - d) * (-i)
+            fz[fpad(base)] = cadd(t0, t2);
+            fz[fpad(base + q)] = cmul(csub(t0, t2), __ldg(&W[2 * j * ts]));
+            fz[fpad(base + 2 * q)] = cmul(cadd(t1, t3), __ldg(&W[j * ts]));
+            fz[fpad(base + 3 * q)] = cmul(csub(t1, t3), __ldg(&W[3 * j * ts]));
+        }
+        __syncthreads();
+    }
+    if (len == 2) {
+        for (int t = tid; t < (P >> 1); t += FFT_THREADS) {
+            const double2 u = fz[fpad(2 * t)], v = fz[fpad(2 * t + 1)];
+            fz[fpad(2 * t)] = cadd(u, v);
+            fz[fpad(2 * t + 1)] = csub(u, v);
+        }
+        __syncthreads();
+    }
+    // filter: the spectrum is in bit-reversed order
+    for (int i = tid; i < P; i += FFT_THREADS) {
+        const double h = __ldg(&H[__brev((unsigned)i) >> (32 - log2P)]);
+        const double2 v = fz[fpad(i)];
+        fz[fpad(i)] = make_double2(v.x * h, v.y * h);
+    }
+    __syncthreads();
+    // inverse: the stages above undone in reverse order, conjugate
+    // twiddles, unnormalised (the result is P times the filtered signal)
+    len = 4;
+    if (log2P & 1) {
+        for (int t = tid; t < (P >> 1); t += FFT_THREADS) {
+            const double2 u = fz[fpad(2 * t)], v = fz[fpad(2 * t + 1)];
+            fz[fpad(2 * t)] = cadd(u, v);
+            fz[fpad(2 * t + 1)] = csub(u, v);
+        }
+        __syncthreads();
+        len = 8;
+    }
+    for (lq = (len == 4 ? 0 : 1); len <= P; len <<= 2, lq += 2) {
+        const int q = len >> 2, ts = P / len;
+        for (int t = tid; t < (P >> 2); t += FFT_THREADS) {
+            const int j = t & (q - 1), base = ((t >> lq) * len) + j;
+            const double2 y0 = fz[fpad(base)];
+            const double2 y2 = cmulc(fz[fpad(base + q)], __ldg(&W[2 * j * ts]));
+            const double2 y1 = cmulc(fz[fpad(base + 2 * q)], __ldg(&W[j * ts]));
+            const double2 y3 = cmulc(fz[fpad(base + 3 * q)], __ldg(&W[3 * j * ts]));
+            const double2 t0 = cadd(y0, y2), t2 = csub(y0, y2), t1 = cadd(y1, y3);
+            const double2 dd = csub(y1, y3);
+            const double2 t3 = make_double2(-dd.y, dd.x);  // (y1 - y3) * i
+            fz[fpad(base)] = cadd(t0, t1);
+            fz[fpad(base + q)] = cadd(t2, t3);
+            fz[fpad(base + 2 * q)] = csub(t0, t1);
+            fz[fpad(base + 3 * q)] = csub(t2, t3);
+        }
+        __syncthreads();
+    }
+    // the first cols values, scaled by 1 / P (exact: P is a power of two)
+    const double inv = 1.0 / (double)P;
+    float* out0 = dst ? (dst_table ? (float*)dst_table[a0] : dst + (int64_t)a0 * da) + (int64_t)r0 * dr : nullptr;
+    float* out1 = dst ? (dst_table ? (float*)dst_table[a1] : dst + (int64_t)a1 * da) + (int64_t)r1 * dr : nullptr;
+    for (int j = tid; j < cols; j += FFT_THREADS) {
+        const double2 v = fz[fpad(j)];
+        const float f0 = __double2float_rn(v.x * inv);
+        if (out0) out0[(int64_t)j * dc] = f0;
+        if (surf) surf2DLayeredwrite(f0, surf, j * (int)sizeof(float), r0, layer0 + a0);
+        if (two) {
+            const float f1 = __double2float_rn(v.y * inv);
+            if (out1) out1[(int64_t)j * dc] = f1;
+            if (surf) surf2DLayeredwrite(f1, surf, j * (int)sizeof(float), r1, layer0 + a1);
+        }
     }
 }
 
@@ -179,4 +332,43 @@ extern "C" int kk_sirt_update(float* x, const float* g, const float* scale, cons
     sirt_update_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(x, g, scale, mask, min_value, max_value,
                                                                          has_min, has_max, n);
     return kk_check_launch("kk_sirt_update");
+}
+
+extern "C" int kk_fdk_filter(const kk_projections* src, const double* geom, const double* H, const double* W,
+                             int64_t P, const kk_projections* dst, kk_layered* tex, int64_t layer0, void* stream) {
+    const char* who = "kk_fdk_filter";
+    int rc = check_f32_projections(src, who);
+    if (rc) return rc;
+    if (!H || !W) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: filter or twiddles are NULL", who);
+    if (P < 64 || P > FFT_MAX_P || (P & (P - 1)))
+        return kk_fail(KK_ERR_UNSUPPORTED, "%s: padded length %lld must be a power of two in [64, %d]", who,
+                       (long long)P, FFT_MAX_P);
+    if (P < 2 * src->cols)
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: padded length %lld shorter than 2*cols", who, (long long)P);
+    if (dst) {
+        rc = check_f32_projections(dst, who);
+        if (rc) return rc;
+        if (dst->n_angles != src->n_angles || dst->rows != src->rows || dst->cols != src->cols)
+            return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: destination shape differs from the source", who);
+    }
+    if (tex) {
+        if (!tex->surf) return kk_fail(KK_ERR_UNSUPPORTED, "%s: texture has no surface", who);
+        if (tex->dtype != KK_F32 || tex->height != src->rows || tex->width != src->cols || layer0 < 0 ||
+            layer0 + src->n_angles > tex->layers)
+            return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: texture layers [%lld, %lld) do not fit", who,
+                           (long long)layer0, (long long)(layer0 + src->n_angles));
+    }
+    const int64_t lines = src->n_angles * src->rows;
+    if (lines > 0x7ffffffe) return kk_fail(KK_ERR_UNSUPPORTED, "%s: too many rows", who);
+    int log2P = 0;
+    while ((1LL << log2P) < P) ++log2P;
+    const size_t smem = sizeof(double2) * (size_t)(P + P / 8);
+    rc = kk_allow_smem((const void*)fdk_filter_kernel, smem, who);
+    if (rc) return rc;
+    fdk_filter_kernel<<<(unsigned)((lines + 1) / 2), FFT_THREADS, smem, (cudaStream_t)stream>>>(
+        (const float*)src->data, src->table, src->stride[0], src->stride[1], src->stride[2], (int)lines,
+        (int)src->rows, (int)src->cols, geom, H, (const double2*)W, (int)P, log2P, dst ? (float*)dst->data : nullptr,
+        dst ? dst->table : nullptr, dst ? dst->stride[0] : 0, dst ? dst->stride[1] : 0, dst ? dst->stride[2] : 0,
+        tex ? tex->surf : 0, (int)layer0);
+    return kk_check_launch(who);
 }

@@ -1,6 +1,8 @@
 // Cone-beam forward projection (ray-driven) for sm_100a: kernel and the
 // kk_cone_fp* entry points of include/kk.h.
+#include "kk_async.cuh"
 #include "kk_cone.cuh"
+#include <climits>
 #include <type_traits>
 
 namespace kk {
@@ -353,6 +355,370 @@ __global__ void __launch_bounds__(32 * FP_COLS, KK_FP_MINBLOCKS) cone_fp_kernel(
     fp_block<TV, TP, TEX8, EPI>(L, blockIdx.x);
 }
 
+// ---------------------------------------------------------------------------
+// forward projection with shared-memory volume tiles
+// ---------------------------------------------------------------------------
+// Rays traced on the CUDA cores whose detector rows share the D1 coordinate
+// (circular scans: the PATH 2 blocks above) sample a tile of each slice
+// staged in shared memory by the tensor-copy unit, instead of four global
+// loads per sample. A block's 8 x 64 rays touch, in every slice, a small
+// window of the volume: BRICK_D1 texels along D1 (8 columns) by BRICK_D2
+// along D2 (64 rows). A ninth, producer warp computes that window exactly
+// and copies it with one TMA tile load per slice into a ring of
+// BRICK_STAGES slots; the eight column warps wait for a slot, sample it
+// with 32-bit shared-memory addressing and release it. Out-of-volume
+// texels of a tile are zero-filled by the copy, which is the border rule
+// of the texture path, so every sample has the value the global-memory
+// code computes, with the same operations: results are bit-identical.
+//
+// The window: along D1 every column's coordinate sequence is replicated
+// bit for bit by a producer lane (exact), along D2 the block's four corner
+// rays bound the others (the D2 coordinate is monotonic in row and column
+// for a planar detector), widened by a texel each side. Each warp checks
+// its own rays against the window before it samples a tile (per slab for
+// D2, per slice for D1); a slice it cannot prove inside (or a window that
+// does not fit a slot) is sampled from global memory with the bounds-
+// checked code instead, so the tile path can never read outside a slot.
+constexpr int BRICK_D1 = 10;  // texels of a tile along D1 (one per column, with margins)
+constexpr int BRICK_D2 = 72;  // texels along D2: 288 bytes, a multiple of 16
+constexpr int BRICK_STAGES = 8;
+constexpr int BRICK_TILE_BYTES = BRICK_D1 * BRICK_D2 * 4;
+constexpr int BRICK_STAGE_FLOATS = (BRICK_TILE_BYTES + 127) / 128 * 32;  // 128-byte aligned slots
+constexpr int BRICK_WARPS = FP_COLS + 1;                                   // + the producer
+#ifndef KK_FP_BRICK_MINBLOCKS
+#define KK_FP_BRICK_MINBLOCKS 5
+#endif
+
+enum BrickMode { BRICK_TILE = 0, BRICK_ZERO = 1, BRICK_GLOBAL = 2 };
+
+struct BrickHdr {
+    int mode;
+    int d1lo, d2lo;    // tile origin (texels) along D1 and D2
+    float zlo, zhi;    // the slab's D2 coordinate range of the corner rays
+    int pad[3];
+};
+
+constexpr size_t BRICK_SMEM = (size_t)BRICK_STAGES * BRICK_STAGE_FLOATS * 4 + BRICK_STAGES * sizeof(BrickHdr) +
+                              2 * BRICK_STAGES * sizeof(uint64_t) + 16;
+
+struct FpBrick {
+    FpArgs L;
+    CUtensorMap map[2];  // slice axis = slowest memory axis [0] or middle axis [1]
+    int ok[3];           // rays along world axis A may use tiles
+};
+
+// timed-out waits since the last kk_wait_timeouts() (0 unless a copy or a
+// barrier failed)
+static __device__ unsigned int g_fp_timeouts;
+
+// The block's dynamic shared memory: BRICK_STAGES tile slots, their
+// headers, the full / empty barrier arrays and an abort flag. Indexed
+// through the array itself so that tile reads are 32-bit shared loads.
+extern __shared__ __align__(128) float brick_sm[];
+
+__device__ __forceinline__ BrickHdr* brick_hdr() {
+    return reinterpret_cast<BrickHdr*>(brick_sm + BRICK_STAGES * BRICK_STAGE_FLOATS);
+}
+__device__ __forceinline__ uint32_t brick_full(int st) {
+    return smem_addr(brick_hdr() + BRICK_STAGES) + 8 * st;
+}
+__device__ __forceinline__ uint32_t brick_empty(int st) {
+    return smem_addr(brick_hdr() + BRICK_STAGES) + 8 * (BRICK_STAGES + st);
+}
+__device__ __forceinline__ volatile int* brick_abort() {
+    return reinterpret_cast<volatile int*>(reinterpret_cast<uint64_t*>(brick_hdr() + BRICK_STAGES) +
+                                           2 * BRICK_STAGES);
+}
+
+__device__ __forceinline__ void brick_timeout() {
+    *brick_abort() = 1;
+    atomicAdd(&g_fp_timeouts, 1u);
+}
+
+// Producer warp: per slice, the tile window and one tensor copy.
+__device__ __forceinline__ void brick_producer(const FpBrick& B, const kk_fp_angle* P, int A, int D1, int D2, int r0,
+                                               int c0, int nw) {
+    const FpArgs& L = B.L;
+    const int lane = threadIdx.x & 31;
+    float src[3], cor[3], u[3], v[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        src[k] = __ldg(&P->src[k]);
+        cor[k] = __ldg(&P->corner[k]);
+        u[k] = __ldg(&P->u[k]);
+        v[k] = __ldg(&P->v[k]);
+    }
+    // lanes 0..7: D1 of column c0 + lane (shared by its rows); lanes 8..15
+    // and 16..23: D2 of the block's first and last row of column c0 + lane % 8
+    const int col = lane & 7;
+    const bool cvalid = col < nw;
+    const int r_last = min(r0 + FP_ROWS_T - 1, L.rows - 1);
+    const RaySetup R = ray_setup(src, cor, u, v, A, D1, D2, lane < 16 ? r0 : r_last, c0 + (cvalid ? col : 0),
+                                 L.os[3 * A + 0], L.os[3 * A + 1]);
+    const bool xl = lane < 8 && cvalid;
+    const bool zl = lane >= 8 && lane < 24 && cvalid;
+    const int nS = L.vn[A], n1 = L.vn[D1], n2 = L.vn[D2];
+    const float half1 = 0.5f * (float)n1, half2 = 0.5f * (float)n2;
+    const bool slow = L.rank[A] == 2;
+    const CUtensorMap* map = &B.map[slow ? 0 : 1];
+    const int s_end = min(nS, L.s_end);
+    int k = 0;
+    bool alive = true;
+    for (int off = L.s_begin; off < s_end && alive; off += L.slab) {
+        const float t1 = __fadd_rn(__fsub_rn((float)off, 0.5f * (float)nS), 0.5f);
+        const int end = min(off + L.slab, nS);
+        float y = __fadd_rn(fmaf(R.a1, t1, R.b1), half1);
+        const float zs = __fadd_rn(fmaf(R.a2, t1, R.b2), half2);
+        const float ze = fmaf(R.a2, (float)(end - 1 - off), zs);
+        // NaN-propagating extremes: a NaN corner makes the window unusable
+        float lo = zl ? (zs < ze ? zs : ze) : COORD_LIMIT, hi = zl ? (zs < ze ? ze : zs) : -COORD_LIMIT;
+#pragma unroll
+        for (int d = 16; d >= 1; d >>= 1) {
+            const float ol = __shfl_xor_sync(0xffffffffu, lo, d), oh = __shfl_xor_sync(0xffffffffu, hi, d);
+            lo = (ol < lo || ol != ol) ? ol : lo;
+            hi = (oh > hi || oh != oh) ? oh : hi;
+        }
+        const bool finite = lo >= -COORD_LIMIT && hi <= COORD_LIMIT;
+        int zlo_i = 0, zhi_i = 0;
+        if (finite) {
+            zlo_i = (int)floorf(lo - 0.5f) - 1;  // texel of the lowest sample, one more below
+            zhi_i = (int)floorf(hi - 0.5f) + 2;  // its right neighbour, one more above
+        }
+        const int z0 = zlo_i & ~3;  // 16-byte aligned start of the copy
+        const bool zfit = finite && zhi_i - z0 < BRICK_D2;
+        const bool zout = finite && (zhi_i < 0 || zlo_i > n2 - 1);
+        for (int sl = off; sl < end; ++sl, ++k) {
+            int xi = INT_MAX, xa = INT_MIN;
+            if (xl) {
+                xi = split_coord<true>(y).i;
+                xa = xi;
+            }
+            y = __fadd_rn(y, R.a1);
+            const int x_lo = __reduce_min_sync(0xffffffffu, xi);
+            const int x_hi = __reduce_max_sync(0xffffffffu, xa) + 1;
+            const bool xout = x_hi < 0 || x_lo > n1 - 1;
+            const int mode = (finite && (zout || xout)) ? BRICK_ZERO
+                             : (zfit && x_hi - x_lo < BRICK_D1) ? BRICK_TILE
+                                                                 : BRICK_GLOBAL;
+            const int st = k % BRICK_STAGES;
+            if (k >= BRICK_STAGES) {
+                bool ok = true;
+                if (lane == 0) ok = mbar_wait(brick_empty(st), ((k / BRICK_STAGES) - 1) & 1) && !*brick_abort();
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                if (!ok) {
+                    if (lane == 0 && !*brick_abort()) brick_timeout();
+                    alive = false;
+                    break;
+                }
+            }
+            if (lane == 0) {
+                BrickHdr h;
+                h.mode = mode;
+                h.d1lo = x_lo;
+                h.d2lo = z0;
+                h.zlo = lo;
+                h.zhi = hi;
+                brick_hdr()[st] = h;
+                if (mode == BRICK_TILE) {
+                    mbar_arrive_expect_tx(brick_full(st), BRICK_TILE_BYTES);
+                    tma_load_3d(smem_addr(brick_sm + st * BRICK_STAGE_FLOATS), map, z0, slow ? x_lo : sl,
+                                slow ? sl : x_lo, brick_full(st));
+                } else {
+                    mbar_arrive(brick_full(st));
+                }
+            }
+            __syncwarp();
+        }
+    }
+    if (!alive && lane == 0) {
+        // let the copies already issued land before the block's shared
+        // memory goes away (bounded as well)
+        for (int j = max(0, k - BRICK_STAGES); j < k; ++j)
+            if (!mbar_wait(brick_full(j % BRICK_STAGES), (j / BRICK_STAGES) & 1)) break;
+    }
+}
+
+// Bounds-checked samples of slice sl from global memory for the two rays
+// of a thread (a window the warp cannot prove its rays inside): the same
+// operations as the tile path, so the same values.
+template <int RULE>
+__device__ __noinline__ float2 brick_global_sample(const FpArgs& L, int A, int D1, int D2, int sl, float y,
+                                                   float2 z2, float2 v2) {
+    const Split ay = split_coord<true>(y);
+    const int n1 = L.vn[D1], n2 = L.vn[D2];
+    const int64_t st1 = L.vs[D1];
+    const float* row0 = (const float*)L.vol + (int64_t)sl * L.vs[A] + (int64_t)ay.i * st1;
+    const bool y0ok = (unsigned)ay.i < (unsigned)n1;
+    const bool y1ok = (unsigned)(ay.i + 1) < (unsigned)n1;
+    v2.x = fast_sample<true, true, RULE>(v2.x, row0, row0 + st1, y0ok, y1ok, n2, ay.w, z2.x);
+    v2.y = fast_sample<true, true, RULE>(v2.y, row0, row0 + st1, y0ok, y1ok, n2, ay.w, z2.y);
+    return v2;
+}
+
+// Column warp: the rays of column c, rows r0 + lane and r0 + lane + 32.
+template <int EPI, int RULE>
+__device__ __forceinline__ void brick_consumer(const FpBrick& B, const kk_fp_angle* P, int a, int A, int D1, int D2,
+                                               int r0, int c, int lane) {
+    static_assert(FP_RPT == 2, "two rays per thread");
+    const FpArgs& L = B.L;
+    float src[3], cor[3], u[3], v[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        src[k] = __ldg(&P->src[k]);
+        cor[k] = __ldg(&P->corner[k]);
+        u[k] = __ldg(&P->u[k]);
+        v[k] = __ldg(&P->v[k]);
+    }
+    const float sc1 = L.os[3 * A + 0], sc2 = L.os[3 * A + 1];
+    const int nS = L.vn[A];
+    auto out_ptr = [&](int k) -> float* {
+        const int64_t off = (int64_t)(r0 + lane + 32 * k) * L.ps[1] + (int64_t)c * L.ps[2];
+        return L.table ? (float*)L.table[a] + off : (float*)L.out + (int64_t)a * L.ps[0] + off;
+    };
+    RaySetup R[2];
+    float acc[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const bool valid = r0 + lane + 32 * k < L.rows;
+        // rows past the detector trace its last row (inside the window)
+        R[k] = ray_setup(src, cor, u, v, A, D1, D2, min(r0 + lane + 32 * k, L.rows - 1), c, sc1, sc2);
+        // the running sum starts from the stored value, as in fp_trace
+        acc[k] = (L.additive && valid) ? ld_rw(out_ptr(k)) : 0.f;
+    }
+    const float a1 = R[0].a1;
+    const float2 a2 = f2(R[0].a2, R[1].a2);
+    const int s_end = min(nS, L.s_end);
+    int k = 0;
+    bool alive = true;
+    for (int off = L.s_begin; off < s_end; off += L.slab) {
+        const float t1 = __fadd_rn(__fsub_rn((float)off, 0.5f * (float)nS), 0.5f);
+        const int end = min(off + L.slab, nS);
+        float y = __fadd_rn(fmaf(R[0].a1, t1, R[0].b1), 0.5f * (float)L.vn[D1]);
+        const float half2 = 0.5f * (float)L.vn[D2];
+        float2 z2 = f2(__fadd_rn(fmaf(R[0].a2, t1, R[0].b2), half2), __fadd_rn(fmaf(R[1].a2, t1, R[1].b2), half2));
+        float2 v2 = f2(0.f);
+        bool slab_ok = false;
+        for (int sl = off; sl < end; ++sl, ++k) {
+            const int st = k % BRICK_STAGES;
+            if (!mbar_wait(brick_full(st), (k / BRICK_STAGES) & 1)) {
+                if (lane == 0) brick_timeout();
+                alive = false;
+                break;
+            }
+            const BrickHdr* h = brick_hdr() + st;
+            const int mode = h->mode;
+            if (sl == off) {
+                // every sample of this slab's rays lies within the window's
+                // D2 range (false for NaN coordinates)
+                const float span = (float)(end - 1 - off);
+                const float ze0 = fmaf(a2.x, span, z2.x), ze1 = fmaf(a2.y, span, z2.y);
+                const float lo = h->zlo - 0.5f, hi = h->zhi + 0.5f;
+                const bool ok = z2.x >= lo && ze0 >= lo && z2.y >= lo && ze1 >= lo && z2.x <= hi && ze0 <= hi &&
+                                z2.y <= hi && ze1 <= hi;
+                slab_ok = __all_sync(0xffffffffu, ok);
+            }
+            const Split ay = split_coord<true>(y);  // shared by the column
+            const int xi = ay.i - h->d1lo;
+            const bool inside = slab_ok && (unsigned)xi <= (unsigned)(BRICK_D1 - 2) && mode != BRICK_GLOBAL;
+            if (inside && mode == BRICK_TILE) {
+                const float S = ay.w;
+                const float S256 = S * (1.f / 256.f);
+                const int rbase = st * BRICK_STAGE_FLOATS + xi * BRICK_D2 - 0x4B4000 - h->d2lo;
+                const float2 mm = add2_rd(fma2_rd(z2, f2(256.f), f2(-127.5f)), f2(12582912.f));
+                const int b0 = __float_as_int(mm.x), b1 = __float_as_int(mm.y);
+                const int o0 = rbase + (b0 >> 8), o1 = rbase + (b1 >> 8);
+                const float2 t00 = f2(brick_sm[o0], brick_sm[o1]);
+                const float2 t10 = f2(brick_sm[o0 + 1], brick_sm[o1 + 1]);
+                const float2 t01 = f2(brick_sm[o0 + BRICK_D2], brick_sm[o1 + BRICK_D2]);
+                const float2 t11 = f2(brick_sm[o0 + BRICK_D2 + 1], brick_sm[o1 + BRICK_D2 + 1]);
+                const float2 Fr = f2(__int_as_float((b0 & 255) | 0x4B000000), __int_as_float((b1 & 255) | 0x4B000000));
+                const float2 F = add2(Fr, f2(-8388608.f));
+                const float2 x1 = add2(add2_rd(fma2(F, f2(S256), f2(0.5f)), f2(12582912.f)), f2(-12582912.f));
+                float2 x0;
+                if (RULE == 1)
+                    x0 = add2(add2_rd(fma2(F, f2(-S256), f2(0.5f)), f2(12582912.f)), add2(Fr, f2(-20971520.f)));
+                else
+                    x0 = sub2(F, x1);
+                v2 = fma2(f2(256.f), t00, v2);
+                v2 = fma2(f2(S), sub2(t01, t00), v2);
+                v2 = fma2(x1, sub2(t11, t01), v2);
+                v2 = fma2(x0, sub2(t10, t00), v2);
+            } else if (!inside) {
+                v2 = brick_global_sample<RULE>(L, A, D1, D2, sl, y, z2, v2);
+            }  // else: every texel of the window is outside the volume
+            z2 = add2(z2, a2);
+            y = __fadd_rn(y, a1);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(brick_empty(st));
+        }
+        if (!alive) break;
+        const float oscale = L.os[3 * A + 2];
+        acc[0] = fmaf(__fmul_rn(__fmul_rn(v2.x, 1.f / 256.f), R[0].corr), oscale, acc[0]);
+        acc[1] = fmaf(__fmul_rn(__fmul_rn(v2.y, 1.f / 256.f), R[1].corr), oscale, acc[1]);
+    }
+    if (!alive) return;  // reported through kk_wait_timeouts; outputs untouched
+#pragma unroll
+    for (int kk2 = 0; kk2 < 2; ++kk2) {
+        const int r = r0 + lane + 32 * kk2;
+        if (r >= L.rows) continue;
+        float out = acc[kk2];
+        if (EPI == FP_RESIDUAL && L.final_pass) {
+            const int64_t e = (int64_t)a * L.ps[0] + (int64_t)r * L.ps[1] + (int64_t)c * L.ps[2];
+            out = __fmul_rn(__fsub_rn(out, ld((const float*)L.res_y + e)), ld((const float*)L.res_w + e));
+        }
+        st(out_ptr(kk2), out);
+    }
+}
+
+// One launch of float32 volume and projections in which blocks whose rays
+// qualify use the tiles; all other blocks run the code of cone_fp_kernel
+// (the producer warp idles there).
+template <int EPI>
+__global__ void __launch_bounds__(32 * BRICK_WARPS, KK_FP_BRICK_MINBLOCKS)
+    cone_fp_brick_kernel(const __grid_constant__ FpBrick B) {
+    const FpArgs& L = B.L;
+    int t = blockIdx.x;
+    const int ct = t % L.col_tiles;
+    t /= L.col_tiles;
+    const int rec = t % L.n_angles;
+    const int rt = t / L.n_angles;
+    const kk_fp_angle* P = L.angles + rec;
+    const int A = __ldg(&P->axis);
+    const int D1 = A == 1 ? 0 : 1;
+    const int D2 = A == 2 ? 0 : 2;
+    const int rule = 2 - L.rank[A];
+    const bool use_tex = L.vtex && L.rank[A] == 2 && !(__ldg(&P->flags) & KK_FP_NO_TEXTURE);
+    const bool shared = __ldg(&P->v[A]) == 0.f && __ldg(&P->v[D1]) == 0.f;
+    if (use_tex || !shared || !B.ok[A] || rule > 1) {
+        if (threadIdx.x < 32 * FP_COLS) fp_block<float, float, true, EPI>(L, blockIdx.x);
+        return;
+    }
+    // a wait of an earlier block gave up: the pipeline is broken, stop
+    // quickly instead of letting every block wait out its budget
+    if (*(volatile unsigned int*)&g_fp_timeouts) return;
+    const int c0 = ct * FP_COLS, r0 = rt * FP_ROWS_T;
+    const int nw = min(FP_COLS, L.cols - c0);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < BRICK_STAGES; ++s) {
+            mbar_init(brick_full(s), 1);
+            mbar_init(brick_empty(s), nw);
+        }
+        *brick_abort() = 0;
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (warp == FP_COLS) {
+        brick_producer(B, P, A, D1, D2, r0, c0, nw);
+    } else if (warp < nw) {
+        const int a = __ldg(&P->index);
+        if (rule == 1)
+            brick_consumer<EPI, 1>(B, P, a, A, D1, D2, r0, c0 + warp, lane);
+        else
+            brick_consumer<EPI, 0>(B, P, a, A, D1, D2, r0, c0 + warp, lane);
+    }
+}
+
 // Many problems in one launch: the argument blocks of up to KK_MAX_BATCH
 // projections travel in the kernel's parameter space (no device memory),
 // each block finds its problem from the prefix block counts and copies that
@@ -393,16 +759,53 @@ using namespace kk;
 // The running float32 sums are carried in the projections between
 // launches: same operations and rounding as one launch.
 constexpr int FP_AUTO_SPAN = 256;
-static int g_fp_span = 0;  // 0: FP_AUTO_SPAN, < 0: one launch, > 0: slices
+// span of the legacy entry points (kk_fp_set_span), per calling thread:
+// 0 = FP_AUTO_SPAN, < 0 = one launch, > 0 = slices
+static thread_local int g_fp_span = 0;
 
-static int fp_span(int nmax, int slab) {
-    const int span = g_fp_span == 0 ? FP_AUTO_SPAN : g_fp_span;
+static int fp_span(int nmax, int slab, int setting) {
+    const int span = setting == 0 ? FP_AUTO_SPAN : setting;
     if (span < 0 || span >= nmax) return 0;
     return (span + slab - 1) / slab * slab;
 }
 
+// Tensor maps of the volume for the shared-memory tile path: float32, the
+// unit-stride axis is the tiles' D2, the other strides multiples of 16
+// bytes and a 16-byte aligned base. False: the path is not available
+// (the kernel then traces with direct loads).
+static bool brick_prepare(FpBrick& B, const FpArgs& L) {
+    int ax_of_rank[3];
+    for (int k = 0; k < 3; ++k) ax_of_rank[L.rank[k]] = k;
+    const int r0 = ax_of_rank[0], r1 = ax_of_rank[1], r2 = ax_of_rank[2];
+    if (L.vs[r0] != 1 || (L.vs[r1] * 4) % 16 != 0 || (L.vs[r2] * 4) % 16 != 0 || ((uintptr_t)L.vol & 15) != 0 ||
+        L.vs[r2] * 4 >= ((int64_t)1 << 40))
+        return false;
+    bool any = false;
+    for (int A = 0; A < 3; ++A) {
+        const int D2 = A == 2 ? 0 : 2;
+        B.ok[A] = A != r0 && D2 == r0;
+        any = any || B.ok[A];
+    }
+    if (!any) return false;
+    const uint64_t dims[3] = {(uint64_t)L.vn[r0], (uint64_t)L.vn[r1], (uint64_t)L.vn[r2]};
+    const uint64_t strides[2] = {(uint64_t)L.vs[r1] * 4, (uint64_t)L.vs[r2] * 4};
+    const uint32_t box_slow[3] = {BRICK_D2, BRICK_D1, 1};  // slices along the slowest axis
+    const uint32_t box_mid[3] = {BRICK_D2, 1, BRICK_D1};   // slices along the middle axis
+    if (kk_encode_tile_map(&B.map[0], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)L.vol, dims, strides, box_slow,
+                           "kk_cone_fp") != KK_OK ||
+        kk_encode_tile_map(&B.map[1], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)L.vol, dims, strides, box_mid,
+                           "kk_cone_fp") != KK_OK)
+        return false;
+    return true;
+}
+
+struct FpLaunch {
+    int span_setting;  // as kk_fp_options.span
+    bool tiles;        // shared-memory tiles where the rays qualify
+};
+
 template <typename TV, typename TP, int EPI>
-static void launch_fp_typed(const FpArgs& base, bool tex8, cudaStream_t s) {
+static void launch_fp_typed(const FpArgs& base, bool tex8, cudaStream_t s, const FpLaunch& opt) {
     FpArgs L = base;
     L.col_tiles = (L.cols + FP_COLS - 1) / FP_COLS;
     const int row_tiles = (L.rows + FP_ROWS_T - 1) / FP_ROWS_T;
@@ -412,8 +815,13 @@ static void launch_fp_typed(const FpArgs& base, bool tex8, cudaStream_t s) {
     // and a residual computed in place (out is y or the weight) needs its
     // operand intact until the last launch: one launch then
     const bool in_place = EPI == FP_RESIDUAL && (L.res_y == L.out || L.res_w == L.out);
-    const int span = std::is_same<TP, float>::value && !in_place ? fp_span(nmax, L.slab) : 0;
+    const int span = std::is_same<TP, float>::value && !in_place ? fp_span(nmax, L.slab, opt.span_setting) : 0;
     const int passes = span ? (nmax + span - 1) / span : 1;
+    // float32 volume and projections with texture-compatible weights may
+    // use the shared-memory tiles
+    FpBrick Bl;
+    const bool brick = std::is_same<TV, float>::value && std::is_same<TP, float>::value && tex8 && opt.tiles &&
+                       brick_prepare(Bl, L);
     for (int p = 0; p < passes; ++p) {
         if (span) {
             L.s_begin = p * span;
@@ -421,18 +829,22 @@ static void launch_fp_typed(const FpArgs& base, bool tex8, cudaStream_t s) {
             L.additive = p == 0 ? base.additive : 1;
             L.final_pass = p == passes - 1;
         }
-        if (tex8)
+        if (brick) {
+            Bl.L = L;
+            cone_fp_brick_kernel<EPI><<<(unsigned)blocks, 32 * BRICK_WARPS, BRICK_SMEM, s>>>(Bl);
+        } else if (tex8) {
             cone_fp_kernel<TV, TP, true, EPI><<<(unsigned)blocks, 32 * FP_COLS, 0, s>>>(L);
-        else
+        } else {
             cone_fp_kernel<TV, TP, false, EPI><<<(unsigned)blocks, 32 * FP_COLS, 0, s>>>(L);
+        }
     }
 }
 
 template <int EPI>
-static int launch_fp(const FpArgs& L, int n_angles, int vdt, int pdt, bool tex8, cudaStream_t s) {
+static int launch_fp(const FpArgs& L, int vdt, int pdt, bool tex8, cudaStream_t s, const FpLaunch& opt) {
 #define KK_FP_CASE(VD, PD, TV, TP)                                   \
     if (vdt == VD && pdt == PD) {                                    \
-        launch_fp_typed<TV, TP, EPI>(L, tex8, s);                    \
+        launch_fp_typed<TV, TP, EPI>(L, tex8, s, opt);               \
         return kk_check_launch("kk_cone_fp");                         \
     }
     KK_FP_CASE(KK_F32, KK_F32, float, float)
@@ -515,6 +927,45 @@ static int check_residual_aliasing(const kk_projections* out, const kk_fp_residu
     return KK_OK;
 }
 
+extern "C" int kk_cone_fp_ex(const kk_volume* vol, const kk_projections* proj, const kk_fp_angle* angles,
+                             const float* out_scale, const kk_fp_options* opts, void* stream) {
+    const char* who = "kk_cone_fp_ex";
+    if (!opts) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: options are NULL", who);
+    if (opts->span < -1) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: span %d", who, opts->span);
+    FpArgs L;
+    int rc = fill_fp_args(L, vol, proj, angles, out_scale, opts->interp, opts->slab, who);
+    if (rc) return rc;
+    const bool tex8 = opts->interp == KK_INTERP_TEX8;
+    if (opts->vtex) {
+        const kk_layered* vtex = opts->vtex;
+        if (!tex8) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: a volume texture needs texture interpolation", who);
+        // the texture holds the volume with one layer per slice of the
+        // slowest axis, rows along the middle axis and columns along the
+        // fastest
+        int ax_of_rank[3];
+        for (int k = 0; k < 3; ++k) ax_of_rank[L.rank[k]] = k;
+        if (vtex->layers != vol->shape[ax_of_rank[2]] || vtex->height != vol->shape[ax_of_rank[1]] ||
+            vtex->width != vol->shape[ax_of_rank[0]])
+            return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: texture extent differs from the volume", who);
+        if ((vol->dtype == KK_F32) != (vtex->dtype == KK_F32))
+            return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: texture and volume storage differ", who);
+        L.vtex = vtex->tex;
+    }
+    L.additive = opts->additive ? 1 : 0;
+    const FpLaunch lo = {opts->span, (opts->flags & KK_FP_OPT_TILES) != 0};
+    if (opts->residual) {
+        const kk_fp_residual* res = opts->residual;
+        if (!res->y || !res->weight) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: residual operands are NULL", who);
+        if (proj->table) return kk_fail(KK_ERR_UNSUPPORTED, "%s: residual epilogue needs strided data", who);
+        rc = check_residual_aliasing(proj, res, who);
+        if (rc) return rc;
+        L.res_y = res->y;
+        L.res_w = res->weight;
+        return launch_fp<FP_RESIDUAL>(L, vol->dtype, proj->dtype, tex8, (cudaStream_t)stream, lo);
+    }
+    return launch_fp<FP_STORE>(L, vol->dtype, proj->dtype, tex8, (cudaStream_t)stream, lo);
+}
+
 extern "C" int kk_fp_set_span(int32_t slices) {
     if (slices < -1) return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_fp_set_span: %d slices", slices);
     g_fp_span = slices;
@@ -524,69 +975,66 @@ extern "C" int kk_fp_set_span(int32_t slices) {
 extern "C" int32_t kk_fp_launches(int32_t max_slices, int32_t slab, int32_t proj_dtype) {
     if (max_slices < 1) return 1;
     const int sl = slab > 0 ? slab : FP_SLAB;
-    const int span = proj_dtype == KK_F32 ? fp_span(max_slices, sl) : 0;
+    const int span = proj_dtype == KK_F32 ? fp_span(max_slices, sl, g_fp_span) : 0;
     return span ? (max_slices + span - 1) / span : 1;
 }
 
+extern "C" int32_t kk_fp_launches_ex(int32_t max_slices, int32_t slab, int32_t proj_dtype, int32_t span) {
+    if (max_slices < 1) return 1;
+    const int sl = slab > 0 ? slab : FP_SLAB;
+    const int sp = proj_dtype == KK_F32 ? fp_span(max_slices, sl, span) : 0;
+    return sp ? (max_slices + sp - 1) / sp : 1;
+}
+
+extern "C" int kk_wait_timeouts(int32_t* count) {
+    if (!count) return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_wait_timeouts: count is NULL");
+    unsigned int n = 0, zero = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(&n, g_fp_timeouts, sizeof(n));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_fp_timeouts, &zero, sizeof(zero));
+    if (e != cudaSuccess) return kk_fail(KK_ERR_CUDA, "kk_wait_timeouts: %s", cudaGetErrorString(e));
+    *count = (int32_t)n;
+    return KK_OK;
+}
+
+// legacy entry points: kk_cone_fp_ex with the calling thread's span
 extern "C" int kk_cone_fp(const kk_volume* vol, const kk_projections* proj, const kk_fp_angle* angles,
                           const float* out_scale, int32_t interp, int32_t slab, int32_t additive, void* stream) {
-    FpArgs L;
-    int rc = fill_fp_args(L, vol, proj, angles, out_scale, interp, slab, "kk_cone_fp");
-    if (rc) return rc;
-    L.additive = additive ? 1 : 0;
-    return launch_fp<FP_STORE>(L, (int)proj->n_angles, vol->dtype, proj->dtype, interp == KK_INTERP_TEX8,
-                               (cudaStream_t)stream);
+    kk_fp_options o = {};
+    o.interp = interp;
+    o.slab = slab;
+    o.additive = additive;
+    o.span = g_fp_span;
+    return kk_cone_fp_ex(vol, proj, angles, out_scale, &o, stream);
 }
 
 extern "C" int kk_cone_fp_residual(const kk_volume* vol, const kk_projections* out, const kk_fp_angle* angles,
                                    const float* out_scale, const kk_fp_residual* residual, int32_t interp,
                                    int32_t slab, void* stream) {
-    FpArgs L;
-    int rc = fill_fp_args(L, vol, out, angles, out_scale, interp, slab, "kk_cone_fp_residual");
-    if (rc) return rc;
     if (!residual || !residual->y || !residual->weight)
         return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_cone_fp_residual: residual operands are NULL");
-    if (out->table)
-        return kk_fail(KK_ERR_UNSUPPORTED, "kk_cone_fp_residual: strided projections only");
-    rc = check_residual_aliasing(out, residual, "kk_cone_fp_residual");
-    if (rc) return rc;
-
-    L.res_y = residual->y;
-    L.res_w = residual->weight;
-    return launch_fp<FP_RESIDUAL>(L, (int)out->n_angles, vol->dtype, out->dtype, interp == KK_INTERP_TEX8,
-                                  (cudaStream_t)stream);
+    if (out && out->table) return kk_fail(KK_ERR_UNSUPPORTED, "kk_cone_fp_residual: strided projections only");
+    kk_fp_options o = {};
+    o.interp = interp;
+    o.slab = slab;
+    o.span = g_fp_span;
+    o.residual = residual;
+    return kk_cone_fp_ex(vol, out, angles, out_scale, &o, stream);
 }
 
 extern "C" int kk_cone_fp_layered(const kk_layered* vtex, const kk_volume* vol, const kk_projections* proj,
                                   const kk_fp_angle* angles, const float* out_scale,
                                   const kk_fp_residual* residual, int32_t slab, int32_t additive, void* stream) {
-    const char* who = "kk_cone_fp_layered";
-    FpArgs L;
-    int rc = fill_fp_args(L, vol, proj, angles, out_scale, KK_INTERP_TEX8, slab, who);
-    if (rc) return rc;
-    if (!vtex) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: texture is NULL", who);
-    // the texture holds the volume with one layer per slice of the slowest
-    // axis, rows along the middle axis and columns along the fastest
-    int ax_of_rank[3];
-    for (int k = 0; k < 3; ++k) ax_of_rank[L.rank[k]] = k;
-    if (vtex->layers != vol->shape[ax_of_rank[2]] || vtex->height != vol->shape[ax_of_rank[1]] ||
-        vtex->width != vol->shape[ax_of_rank[0]])
-        return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: texture extent differs from the volume", who);
-    if ((vol->dtype == KK_F32) != (vtex->dtype == KK_F32))
-        return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: texture and volume storage differ", who);
-    L.vtex = vtex->tex;
-    L.additive = additive ? 1 : 0;
-    if (residual) {
-        if (!residual->y || !residual->weight)
-            return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: residual operands are NULL", who);
-        if (proj->table) return kk_fail(KK_ERR_UNSUPPORTED, "%s: residual epilogue needs strided data", who);
-        rc = check_residual_aliasing(proj, residual, who);
-        if (rc) return rc;
-        L.res_y = residual->y;
-        L.res_w = residual->weight;
-        return launch_fp<FP_RESIDUAL>(L, (int)proj->n_angles, vol->dtype, proj->dtype, true, (cudaStream_t)stream);
-    }
-    return launch_fp<FP_STORE>(L, (int)proj->n_angles, vol->dtype, proj->dtype, true, (cudaStream_t)stream);
+    if (!vtex) return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_cone_fp_layered: texture is NULL");
+    if (residual && (!residual->y || !residual->weight))
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_cone_fp_layered: residual operands are NULL");
+    kk_fp_options o = {};
+    o.interp = KK_INTERP_TEX8;
+    o.slab = slab;
+    o.additive = residual ? 0 : additive;
+    o.span = g_fp_span;
+    o.vtex = vtex;
+    o.residual = residual;
+    return kk_cone_fp_ex(vol, proj, angles, out_scale, &o, stream);
 }
 
 extern "C" int kk_cone_fp_batched(const kk_fp_problem* pr, int32_t n, int32_t interp, int32_t slab, void* stream) {

@@ -44,6 +44,18 @@ class kk_fp_residual(ctypes.Structure):
     _fields_ = [("y", ctypes.c_void_p), ("weight", ctypes.c_void_p)]
 
 
+class kk_fp_options(ctypes.Structure):
+    _fields_ = [("interp", ctypes.c_int32), ("slab", ctypes.c_int32),
+                ("additive", ctypes.c_int32), ("span", ctypes.c_int32),
+                ("flags", ctypes.c_int32), ("vtex", ctypes.c_void_p),
+                ("residual", ctypes.c_void_p)]
+
+
+#: kk_fp_options.flags: shared-memory tiles staged by the tensor-copy
+#: unit instead of direct loads for CUDA-core rays
+KK_FP_OPT_TILES = 1
+
+
 class kk_bp_update(ctypes.Structure):
     _fields_ = [("scale", ctypes.c_void_p), ("mask", ctypes.c_void_p),
                 ("min_value", ctypes.c_float), ("max_value", ctypes.c_float),
@@ -80,7 +92,9 @@ BP_ANGLE_DTYPE = np.dtype([("num_u", "<f4", 4), ("num_v", "<f4", 4),
                            ("den", "<f4", 4)])
 
 #: every symbol include/kk.h declares
-EXPORTS = ("kk_cone_fp", "kk_cone_fp_residual", "kk_cone_fp_layered",
+EXPORTS = ("kk_cone_fp_ex", "kk_fp_launches_ex", "kk_wait_timeouts",
+           "kk_fdk_filter",
+           "kk_cone_fp", "kk_cone_fp_residual", "kk_cone_fp_layered",
            "kk_cone_fp_adjoint", "kk_cone_fp_batched",
            "kk_cone_bp_layered_batched",
            "kk_cone_bp", "kk_cone_bp_static",
@@ -111,6 +125,10 @@ def load():
     vp = ctypes.c_void_p
     P = ctypes.POINTER
     i32, i64, f32 = ctypes.c_int32, ctypes.c_int64, ctypes.c_float
+    L.kk_cone_fp_ex.argtypes = [P(kk_volume), P(kk_projections), vp, vp,
+                                P(kk_fp_options), vp]
+    L.kk_fp_launches_ex.argtypes = [i32, i32, i32, i32]
+    L.kk_wait_timeouts.argtypes = [P(i32)]
     L.kk_cone_fp.argtypes = [P(kk_volume), P(kk_projections), vp, vp, i32,
                              i32, i32, vp]
     L.kk_cone_fp_residual.argtypes = [P(kk_volume), P(kk_projections), vp, vp,
@@ -135,6 +153,8 @@ def load():
                                             P(kk_bp_update), vp, vp]
     L.kk_preweight.argtypes = [P(kk_projections), vp, vp]
     L.kk_filter_rows.argtypes = [P(kk_projections), vp, i64, vp]
+    L.kk_fdk_filter.argtypes = [P(kk_projections), vp, vp, vp, i64,
+                                P(kk_projections), vp, i64, vp]
     L.kk_reciprocal.argtypes = [vp, i64, vp]
     L.kk_sirt_update.argtypes = [vp, vp, vp, vp, f32, f32, i32, i32, i64, vp]
     L.kk_fp_set_span.argtypes = [i32]
@@ -147,6 +167,14 @@ def load():
     L.kk_abi_version.argtypes = []
     _lib = L
     return L
+
+
+def wait_timeouts() -> int:
+    """Waits inside the library's kernels on the current device that gave
+    up since the previous call (0 in normal operation). Synchronous."""
+    n = ctypes.c_int32(0)
+    check(load().kk_wait_timeouts(ctypes.byref(n)))
+    return int(n.value)
 
 
 def check(rc: int) -> None:

@@ -169,7 +169,10 @@ def _streamed_bp(projections: np.ndarray, projection_geometry,
         pw = t.from_numpy(processing.preweight_params(
             projection_geometry)).cuda()
         P = processing.padded_length(cols)
-        h = processing._device_filter(P, filter)
+        if P <= processing.FFT_MAX_P:
+            H, W = processing.device_spectrum(P, filter)
+        else:
+            h = processing._device_filter(P, filter)
     if st.get("last") is not None:
         # the ring's previous user may run on another stream
         cs.wait_event(st["last"])
@@ -179,10 +182,24 @@ def _streamed_bp(projections: np.ndarray, projection_geometry,
         src = t.from_numpy(projections)
     else:
         src = _arrays.as_tensor(projections)
-        if filter is not None:
-            whole = _native.projections_desc(src)
-            _native.check(L.kk_preweight(whole, pw.data_ptr(), stream))
-            _native.check(L.kk_filter_rows(whole, h.data_ptr(), P, stream))
+
+    def fill(tex, chunk, a, in_place):
+        """Pre-weight, filter and store one chunk into its texture in one
+        pass (device input is also rewritten in place, as the reference
+        pre-processes it), or copy it when there is no filter."""
+        if filter is None:
+            tex.copy_from(chunk)
+            return
+        d = _native.projections_desc(chunk)
+        if P > processing.FFT_MAX_P:  # rows beyond the FFT's reach
+            _native.check(L.kk_preweight(d, pw.data_ptr() + a * 13 * 8,
+                                         stream))
+            _native.check(L.kk_filter_rows(d, h.data_ptr(), P, stream))
+            tex.copy_from(chunk)
+            return
+        _native.check(L.kk_fdk_filter(
+            d, pw.data_ptr() + a * 13 * 8, H.data_ptr(), W.data_ptr(), P,
+            d if in_place else None, tex.handle, 0, stream))
     staged, used = [None, None], [None, None]
     for c, a in enumerate(range(0, n, _CHUNK)):
         m, b = min(_CHUNK, n - a), c & 1
@@ -192,7 +209,7 @@ def _streamed_bp(projections: np.ndarray, projection_geometry,
                     for _ in range(2)]
             st["tex"][m] = texs
         if not on_host:
-            texs[b].copy_from(src[a:a + m])
+            fill(texs[b], src[a:a + m], a, True)
             _native.check(L.kk_cone_bp_layered(
                 texs[b].handle, vdesc, params + a * 12 * 4, vox_vol,
                 int(c > 0), 0, stream))
@@ -209,12 +226,7 @@ def _streamed_bp(projections: np.ndarray, projection_geometry,
             staged[b] = t.cuda.Event()
             staged[b].record(st["copy"])
         cs.wait_event(staged[b])
-        pdesc = _native.projections_desc(dev)
-        if filter is not None:
-            _native.check(L.kk_preweight(pdesc, pw.data_ptr() + a * 13 * 8,
-                                         stream))
-            _native.check(L.kk_filter_rows(pdesc, h.data_ptr(), P, stream))
-        texs[b].copy_from(dev)
+        fill(texs[b], dev, a, False)
         used[b] = t.cuda.Event()
         used[b].record(cs)
         _native.check(L.kk_cone_bp_layered(

@@ -10,6 +10,7 @@ memory capped at ``max_projs`` angles; here there is no cap).
 from __future__ import annotations
 
 import copy
+import ctypes
 from typing import Sequence
 
 import numpy as np
@@ -116,6 +117,14 @@ class RayDrivenConeFP(BaseKernel):
     #: let 16-bit volumes use a float16 layered texture (reduced-precision
     #: filtering: for 16-bit storage runs, whose tolerance is the storage's)
     half_texture = False
+    #: slices of every ray's own axis traced per launch (None: the module
+    #: default of ``set_slices_per_launch``; -1: one launch)
+    slices_per_launch = None
+    #: rays traced on the CUDA cores sample shared-memory tiles of the
+    #: volume staged by the tensor-copy unit instead of loading it
+    #: directly (same results bit for bit; slower at the measured shapes,
+    #: so off by default)
+    use_tiles = False
 
     def __init__(self, pixels_per_block: tuple = None,
                  slices_per_block: int = None,
@@ -382,19 +391,30 @@ class RayDrivenConeFP(BaseKernel):
                 f"match the detector {int(det.rows[0])}x{int(det.cols[0])}.")
         osc = np.asarray(self._output_scale(volume_geometry.voxel_size),
                          np.float32).reshape(9)
-        L = _native.load()
         lay = self._volume_texture(vol, vdesc)
-        if lay is not None:
-            _native.check(L.kk_cone_fp_layered(
-                lay.handle, vdesc, pdesc, self._params_dev.data_ptr(),
-                osc.ctypes.data, None, self.slices_per_block,
-                int(bool(additive)), _native.current_stream()))
-        else:
-            _native.check(L.kk_cone_fp(
-                vdesc, pdesc, self._params_dev.data_ptr(), osc.ctypes.data,
-                self._interp, self.slices_per_block, int(bool(additive)),
-                _native.current_stream()))
+        self._launch(vdesc, pdesc, osc, lay, None, additive)
         del keep
+
+    def _options(self, lay, residual, additive) -> "_native.kk_fp_options":
+        o = _native.kk_fp_options()
+        o.interp = self._interp if lay is None else _native.KK_INTERP_TEX8
+        o.slab = self.slices_per_block
+        o.additive = int(bool(additive))
+        o.span = int(_DEFAULT_SPAN if self.slices_per_launch is None
+                     else self.slices_per_launch)
+        o.flags = _native.KK_FP_OPT_TILES if self.use_tiles else 0
+        o.vtex = None if lay is None else lay.handle
+        o.residual = (None if residual is None
+                      else ctypes.cast(ctypes.pointer(residual),
+                                       ctypes.c_void_p))
+        return o
+
+    def _launch(self, vdesc, pdesc, osc, lay, residual, additive):
+        o = self._options(lay, residual, additive)
+        _native.check(_native.load().kk_cone_fp_ex(
+            vdesc, pdesc, self._params_dev.data_ptr(), osc.ctypes.data, o,
+            _native.current_stream()))
+        del residual
 
     #: bytes of ray set-ups the exact adjoint keeps at once (angles are
     #: processed in chunks that fit, recomputing set-ups per chunk)
@@ -464,32 +484,33 @@ class RayDrivenConeFP(BaseKernel):
         osc = np.asarray(self._output_scale(volume_geometry.voxel_size),
                          np.float32).reshape(9)
         lay = self._volume_texture(volume, vdesc)
-        if lay is not None:
-            _native.check(_native.load().kk_cone_fp_layered(
-                lay.handle, vdesc, pdesc, self._params_dev.data_ptr(),
-                osc.ctypes.data, res, self.slices_per_block, 0,
-                _native.current_stream()))
-            return
-        _native.check(_native.load().kk_cone_fp_residual(
-            vdesc, pdesc, self._params_dev.data_ptr(), osc.ctypes.data, res,
-            self._interp, self.slices_per_block, _native.current_stream()))
+        self._launch(vdesc, pdesc, osc, lay, res, False)
+
+
+#: span of projectors whose ``slices_per_launch`` is None
+_DEFAULT_SPAN = 0
 
 
 def set_slices_per_launch(slices: int = 0) -> None:
     """How many slices of every ray's own slice axis one forward-projection
-    launch traces (float32 projections): 0 = the default (256), -1 = the
+    launch traces (float32 projections) for projectors that do not set
+    ``slices_per_launch`` themselves: 0 = the default (256), -1 = the
     whole ray in one launch. Results are the same bit for bit; shorter
-    spans keep the volume band each launch reads in L2. Process-wide."""
-    _native.check(_native.load().kk_fp_set_span(int(slices)))
+    spans keep the volume band each launch reads in L2."""
+    global _DEFAULT_SPAN
+    if int(slices) < -1:
+        raise ValueError(f"slices must be >= -1, got {slices}")
+    _DEFAULT_SPAN = int(slices)
 
 
 def launches_per_projection(max_slices: int, slab: int = 16,
-                            float32: bool = True) -> int:
+                            float32: bool = True, span: int = None) -> int:
     """Kernel launches of one forward projection of a volume whose longest
     axis has ``max_slices`` voxels."""
-    return int(_native.load().kk_fp_launches(
+    return int(_native.load().kk_fp_launches_ex(
         int(max_slices), int(slab),
-        _native.KK_F32 if float32 else _native.KK_F16))
+        _native.KK_F32 if float32 else _native.KK_F16,
+        int(_DEFAULT_SPAN if span is None else span)))
 
 
 __all__ = ["RayDrivenConeFP", "ConeFPParams", "set_slices_per_launch",

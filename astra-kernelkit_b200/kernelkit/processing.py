@@ -1,9 +1,11 @@
 """FDK pre-processing: cone-beam pre-weighting and detector-row filtering.
 
 Mirrors ``kernelkit/processing.py`` of the reference. Both steps run as
-CUDA kernels in float64 (``kk_preweight``, ``kk_filter_rows``) and update
-the projections in place, as the reference does. NumPy input is processed
-on the device and written back.
+CUDA kernels in float64 (``kk_preweight``; ``kk_fdk_filter``, a float64
+FFT filter as the reference's, or ``kk_filter_rows``, a direct circular
+convolution, for padded rows beyond 8192) and update the projections in
+place, as the reference does. NumPy input is processed on the device and
+written back. FDK fuses both with the texture store (``kk_fdk_filter``).
 """
 from __future__ import annotations
 
@@ -60,12 +62,29 @@ def impulse_response(num: int, filter_name: str = "ramlak") -> np.ndarray:
 
 _DEVICE_FILTERS: dict = {}
 
+#: largest padded length the one-pass FFT filter (kk_fdk_filter) handles
+FFT_MAX_P = 8192
+
 
 def _device_filter(num, name):
     key = (num, name.lower())
     if key not in _DEVICE_FILTERS:
         t = _arrays.torch()
         _DEVICE_FILTERS[key] = t.from_numpy(impulse_response(num, name)).cuda()
+    return _DEVICE_FILTERS[key]
+
+
+def device_spectrum(num, name):
+    """(H, W) on the device for ``kk_fdk_filter``: the frequency response
+    of the filter (float64, length ``num``) and the FFT twiddles
+    exp(-2 pi i k / num) as interleaved float64 pairs."""
+    key = ("spectrum", num, name.lower())
+    if key not in _DEVICE_FILTERS:
+        t = _arrays.torch()
+        H = np.ascontiguousarray(_filter(num, name), np.float64)
+        W = np.exp(-2j * np.pi * np.arange(num) / num)
+        W = np.ascontiguousarray(np.stack([W.real, W.imag], axis=1))
+        _DEVICE_FILTERS[key] = (t.from_numpy(H).cuda(), t.from_numpy(W).cuda())
     return _DEVICE_FILTERS[key]
 
 
@@ -107,9 +126,16 @@ def filter(projections, verbose: bool = False, filter: str = "ramlak"):
     the filter's impulse response, in float64."""
     desc, keep, writeback = _as_stack(projections)
     P = padded_length(int(desc.cols))
-    h = _device_filter(P, filter)
-    _native.check(_native.load().kk_filter_rows(desc, h.data_ptr(), P,
-                                                _native.current_stream()))
+    if P <= FFT_MAX_P:
+        # float64 FFT filtering in one pass, as the reference (cuFFT)
+        H, W = device_spectrum(P, filter)
+        _native.check(_native.load().kk_fdk_filter(
+            desc, None, H.data_ptr(), W.data_ptr(), P, desc, None, 0,
+            _native.current_stream()))
+    else:  # direct circular convolution with the impulse response
+        h = _device_filter(P, filter)
+        _native.check(_native.load().kk_filter_rows(
+            desc, h.data_ptr(), P, _native.current_stream()))
     writeback()
     del keep
 

@@ -304,6 +304,53 @@ def load_traffic(workload, kernel):
         return None
 
 
+def run_fdk(pgs, vg, sino, t_bp, reps=3):
+    """FDK (pre-weighting, Ram-Lak filtering, backprojection) of the
+    workload's own sinogram: device-resident input (pre-processed in place
+    as the reference does, so every repetition starts from a fresh copy,
+    outside the timed region), CUDA events around the chunked pipeline;
+    and end to end through ``kk.fdk`` from a host array to a host result
+    (wall clock, synchronised)."""
+    import torch
+
+    import kernelkit as kk
+    from kernelkit import algo
+
+    work = torch.empty_like(sino)
+    ms = []
+    for k in range(reps + 1):
+        work.copy_(sino)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        vol = algo._streamed_bp(work, pgs, vg, "ramlak")
+        b.record()
+        torch.cuda.synchronize()
+        if k:
+            ms.append(a.elapsed_time(b))
+        del vol
+    del work
+    host = sino.cpu().numpy()
+    kk.fdk(host, pgs, vg)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rec = kk.fdk(host, pgs, vg)
+    torch.cuda.synchronize()
+    e2e = (time.perf_counter() - t0) * 1e3
+    del rec, host
+    torch.cuda.empty_cache()
+    dev = statistics.median(ms)
+    return {"ms": dev, "bp_ms": t_bp, "over_bp_ms": dev - t_bp,
+            "e2e_host_ms": e2e,
+            "pipeline": "per 32-angle chunk: one kernel pre-weights, "
+                        "filters (float64 FFT) and writes the chunk into "
+                        "its layered texture, then the BP launch",
+            "timing": f"device input: CUDA events, median of {reps} after "
+                      "one warm-up; e2e: host array in, pinned host "
+                      "volume out, wall clock"}
+
+
 def run_sirt(workload="config2", iters=50):
     """SIRT it/s on a noisy scan (config 2: 256^3, 360 angles, 384^2,
     40 ellipsoids, exact FP64 line integrals with Poisson noise at 1e4
@@ -865,6 +912,12 @@ def run_ours(args):
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unit": UNIT, "cores": cores,
                    "kind": "port", "error": f"{type(e).__name__}: {e}"[:300]}
+    fdk = None
+    if rank == 0 and world == 1 and not args.no_fdk:
+        try:
+            fdk = run_fdk(pgs, vg, proj, t_bp)
+        except Exception as e:  # noqa: BLE001
+            fdk = {"error": f"{type(e).__name__}: {e}"[:300]}
     sirt = batched = None
     if rank == 0 and world == 1 and not args.no_sirt:
         # secondary measurements: a failure here is reported in the line
@@ -898,7 +951,7 @@ def run_ours(args):
             "kernels": kernels, "reference_kernels": refk,
             # per step: one FP launch and one BP launch per 32-angle chunk
             "gpu_launches": args.steps * (fp_launches + (len(pgs) + 31) // 32),
-            "clocks": clocks, "sirt": sirt, "batched": batched,
+            "clocks": clocks, "fdk": fdk, "sirt": sirt, "batched": batched,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -958,6 +1011,8 @@ def main(argv=None):
                     default="headline")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fdk", action="store_true",
+                    help="skip the FDK timing")
     ap.add_argument("--no-reference-kernels", action="store_true",
                     help="skip timing the reference's own CUDA kernels")
     ap.add_argument("--sirt-config5", action="store_true",

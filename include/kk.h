@@ -156,19 +156,68 @@ KK_API int kk_cone_fp_layered(const kk_layered* vtex, const kk_volume* vol,
                               const kk_fp_residual* residual, int32_t slab,
                               int32_t additive, void* stream);
 
-/* Launch split of the three entry points above (no counterpart in the
- * reference, whose FP is one launch): with float32 projections a
- * projection is traced in launches of `slices` slices of every ray's own
- * slice axis (a multiple of the slab; the running float32 sums are carried
- * in the projections, so the result is bit for bit that of one launch)
- * and each launch reads a band of the volume that stays in L2. slices = 0
- * restores the default (256), -1 selects one launch. Process-wide. */
+/* Options of kk_cone_fp_ex. A zero-initialised struct selects the
+ * defaults: texture-compatible weights, 16-slice slabs, overwrite, 256-
+ * slice spans, direct loads, no volume texture, no epilogue. */
+typedef struct {
+    int32_t interp;     /* kk_interp */
+    int32_t slab;       /* slices per coordinate restart; <= 0 selects 16 */
+    int32_t additive;   /* 0: proj = A vol, 1: proj += A vol */
+    int32_t span;       /* launch split (no counterpart in the reference,
+                           whose FP is one launch): with float32 projections
+                           a projection is traced in launches of `span`
+                           slices of every ray's own slice axis (rounded up
+                           to the slab; the running float32 sums are carried
+                           in the projections, so the result is bit for bit
+                           that of one launch) and each launch reads a band
+                           of the volume that stays in L2. 0: 256 slices,
+                           -1: one launch */
+    int32_t flags;      /* KK_FP_OPT_* bits */
+    const kk_layered* vtex;          /* NULL, or a layered copy of the
+                                        volume as for kk_cone_fp_layered */
+    const kk_fp_residual* residual;  /* NULL, or the SIRT epilogue as for
+                                        kk_cone_fp_residual */
+} kk_fp_options;
+
+/* kk_fp_options.flags: rays traced on the CUDA cores sample shared-memory
+ * tiles of each slice staged by the tensor-copy unit instead of loading
+ * the volume directly (same results bit for bit). Off by default: at the
+ * measured shapes the per-slice pipeline costs more instructions than the
+ * loads it replaces. */
+#define KK_FP_OPT_TILES 1
+
+/* The forward projection with every option per call: kk_cone_fp,
+ * kk_cone_fp_residual and kk_cone_fp_layered are this entry point with
+ * the calling thread's kk_fp_set_span. With KK_FP_OPT_TILES, float32
+ * volumes with float32 projections and texture-compatible weights trace
+ * the rays that step along a non-unit-stride axis, whose detector rows
+ * share their in-slice coordinate (circular orbits), from shared-memory
+ * tiles of each slice staged by the tensor-copy unit (needs the volume's
+ * unit-stride axis, 16-byte aligned base and strides); other rays and
+ * other storage use direct loads or the texture. */
+KK_API int kk_cone_fp_ex(const kk_volume* vol, const kk_projections* proj,
+                         const kk_fp_angle* angles, const float* out_scale,
+                         const kk_fp_options* opts, void* stream);
+
+/* Launch split of kk_cone_fp, kk_cone_fp_residual and kk_cone_fp_layered,
+ * as kk_fp_options.span, for the calling thread (each thread starts with
+ * 0 = 256 slices; -1 selects one launch). */
 KK_API int kk_fp_set_span(int32_t slices);
 
 /* Number of kernel launches kk_cone_fp* makes for a volume whose longest
- * axis has max_slices voxels, with this slab and projection dtype. */
+ * axis has max_slices voxels, with this slab and projection dtype, at the
+ * calling thread's span (kk_fp_launches) or a given span (_ex). */
 KK_API int32_t kk_fp_launches(int32_t max_slices, int32_t slab,
                               int32_t proj_dtype);
+KK_API int32_t kk_fp_launches_ex(int32_t max_slices, int32_t slab,
+                                 int32_t proj_dtype, int32_t span);
+
+/* Number of waits inside the library's kernels on the current device that
+ * gave up since the previous call (and resets it): the shared-memory tile
+ * pipeline bounds every wait on a copy or a slot (about a second) and a
+ * kernel whose wait runs out stops and leaves its outputs unwritten
+ * instead of hanging. 0 in normal operation. Synchronous. */
+KK_API int kk_wait_timeouts(int32_t* count);
 
 /* Exact adjoint (transpose) of kk_cone_fp for the same records,
  * out_scale, interp and slab: vol = A^T proj (additive=0) or vol += A^T
@@ -313,6 +362,24 @@ KK_API int kk_preweight(const kk_projections* proj, const double* geom,
  * frequency-domain filter. */
 KK_API int kk_filter_rows(const kk_projections* proj, const double* h, int64_t P,
                    void* stream);
+
+/* FDK pre-processing in one pass (replaces processing.preweight,
+ * processing.py:149-188, followed by processing.filter, processing.py:
+ * 96-126, and the copy into the backprojector's texture): every detector
+ * row of src is pre-weighted as kk_preweight does (geom as there; NULL
+ * skips the weighting), zero-padded to P values, filtered with the
+ * frequency response H (P doubles, real and even, as the reference builds
+ * it) by a float64 FFT (forward, product, inverse, as the reference does
+ * with cuFFT), and its first cols values are stored as float32 into dst
+ * (NULL: not stored; dst may be src itself) and into layers [layer0,
+ * layer0 + n_angles) of tex (NULL: not stored; a float32 kk_layered of
+ * the same rows and cols). W: P complex doubles (re, im) with W[k] =
+ * exp(-2 pi i k / P). P is a power of two in [64, 8192], at least 2 cols;
+ * float32 data. */
+KK_API int kk_fdk_filter(const kk_projections* src, const double* geom,
+                         const double* H, const double* W, int64_t P,
+                         const kk_projections* dst, kk_layered* tex,
+                         int64_t layer0, void* stream);
 
 /* ---- elementwise helpers -------------------------------------------- */
 
