@@ -44,14 +44,19 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t byt
                  : "memory");
 }
 
+// one test of the phase; a warp whose phase is not complete yet sleeps up
+// to WAIT_SUSPEND_NS (woken early when the phase completes) instead of
+// spinning on the issue slots the working warps need
+constexpr uint32_t WAIT_SUSPEND_NS = 2000;
+
 __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(done)
-        : "r"(bar), "r"(parity)
+        : "r"(bar), "r"(parity), "n"(WAIT_SUSPEND_NS)
         : "memory");
     return done != 0;
 }

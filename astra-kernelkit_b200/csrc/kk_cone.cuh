@@ -56,6 +56,12 @@ struct FpArgs {
     // rounding) only in the launch whose final_pass is set
     int s_begin, s_end;
     int final_pass;
+    // 16-bit projections traced in several launches: the float32 running
+    // sums of this launch's records (record-major, rows x cols each) pass
+    // between launches here instead of through the output
+    float* sums;
+    int load_sums;   // start from sums (later launches)
+    int store_sums;  // leave the sums there (all but the last launch)
 };
 
 struct BpArgs {

@@ -104,14 +104,37 @@ __global__ void __launch_bounds__(FILT_BLOCK)
 //
 // The transform runs in shared memory in float64: decimation-in-frequency
 // radix-4 stages (and one radix-2 stage when log2 P is odd) leave the
-// spectrum in bit-reversed order, the multiplication by H reads H at the
-// bit-reversed index, and the inverse stages (conjugate twiddles, in
+// spectrum in bit-reversed order, the multiplication by H uses H in
+// bit-reversed order, and the inverse stages (conjugate twiddles, in
 // reverse order) take bit-reversed input back to natural order, so no
-// permutation pass is needed. W[k] = exp(-2 pi i k / P), k < P, comes from
-// the caller. Shared-memory index i is stored at i + i / 8 to spread the
-// strided accesses of the short stages over the banks.
+// permutation pass is needed. Shared-memory index i is stored at i + i / 8
+// to spread the strided accesses of the short stages over the banks.
+//
+// The plan (kk_fdk_plan, 3 P doubles) holds what the kernel reads, laid
+// out for coalesced loads: H[bitrev(i)] for i < P, then per radix-4 stage
+// of length len (P, P/4, ... down to 4) and j < len / 4 the twiddle W^j
+// (W = exp(-2 pi i / len)) as two doubles; W^2j and W^3j are formed from
+// it in registers (the kernel is bound by its loads and stores, not by
+// float64 arithmetic).
 constexpr int FFT_THREADS = 256;
 constexpr int FFT_MAX_P = 8192;
+
+__global__ void fdk_plan_kernel(double* plan, const double* __restrict__ H, int P, int log2P) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < P) plan[i] = H[__brev((unsigned)i) >> (32 - log2P)];
+    // twiddle records of every stage
+    int off = P;
+    for (int len = P; len >= 4; len >>= 2) {
+        const int q = len >> 2;
+        if (i < q) {
+            double s1, c1;
+            sincospi(-2.0 * (double)i / (double)len, &s1, &c1);
+            plan[off + 2 * i] = c1;
+            plan[off + 2 * i + 1] = s1;
+        }
+        off += 2 * q;
+    }
+}
 
 __device__ __forceinline__ int fpad(int i) { return i + (i >> 3); }
 
@@ -142,8 +165,8 @@ __device__ __forceinline__ double fdk_load(const float* row, int64_t sc, int c, 
 
 __global__ void __launch_bounds__(FFT_THREADS)
     fdk_filter_kernel(const float* src, const uint64_t* src_table, int64_t sa, int64_t sr, int64_t sc, int n_lines,
-                      int rows, int cols, const double* __restrict__ geom, const double* __restrict__ H,
-                      const double2* __restrict__ W, int P, int log2P, float* dst, const uint64_t* dst_table,
+                      int rows, int cols, const double* __restrict__ geom, const double* __restrict__ plan,
+                      int P, int log2P, float* dst, const uint64_t* dst_table,
                       int64_t da, int64_t dr, int64_t dc, cudaSurfaceObject_t surf, int layer0) {
     extern __shared__ double2 fz[];
     const int tid = threadIdx.x;
@@ -165,20 +188,22 @@ __global__ void __launch_bounds__(FFT_THREADS)
     }
     __syncthreads();
     // forward: radix-4 decimation in frequency, then radix 2 if log2 P is odd
+    const double2* tw = reinterpret_cast<const double2*>(plan + P);  // stage records
     int len = P, lq = log2P - 2;  // lq = log2(len / 4)
-    for (; len >= 4; len >>= 2, lq -= 2) {
-        const int q = len >> 2, ts = P / len;
+    for (; len >= 4; tw += (len >> 2), len >>= 2, lq -= 2) {
+        const int q = len >> 2;
         for (int t = tid; t < (P >> 2); t += FFT_THREADS) {
             const int j = t & (q - 1), base = ((t >> lq) * len) + j;
             const double2 a = fz[fpad(base)], b = fz[fpad(base + q)], c = fz[fpad(base + 2 * q)],
                           d = fz[fpad(base + 3 * q)];
+            const double2 w1 = __ldg(&tw[j]), w2 = cmul(w1, w1), w3 = cmul(w2, w1);
             const double2 t0 = cadd(a, c), t1 = csub(a, c), t2 = cadd(b, d);
             const double2 bd = csub(b, d);
             const double2 t3 = make_double2(bd.y, -bd.x);  // (b - d) * (-i)
             fz[fpad(base)] = cadd(t0, t2);
-            fz[fpad(base + q)] = cmul(csub(t0, t2), __ldg(&W[2 * j * ts]));
-            fz[fpad(base + 2 * q)] = cmul(cadd(t1, t3), __ldg(&W[j * ts]));
-            fz[fpad(base + 3 * q)] = cmul(csub(t1, t3), __ldg(&W[3 * j * ts]));
+            fz[fpad(base + q)] = cmul(csub(t0, t2), w2);
+            fz[fpad(base + 2 * q)] = cmul(cadd(t1, t3), w1);
+            fz[fpad(base + 3 * q)] = cmul(csub(t1, t3), w3);
         }
         __syncthreads();
     }
@@ -190,9 +215,9 @@ __global__ void __launch_bounds__(FFT_THREADS)
         }
         __syncthreads();
     }
-    // filter: the spectrum is in bit-reversed order
+    // filter: the spectrum and the plan's H are in bit-reversed order
     for (int i = tid; i < P; i += FFT_THREADS) {
-        const double h = __ldg(&H[__brev((unsigned)i) >> (32 - log2P)]);
+        const double h = __ldg(&plan[i]);
         const double2 v = fz[fpad(i)];
         fz[fpad(i)] = make_double2(v.x * h, v.y * h);
     }
@@ -209,14 +234,17 @@ __global__ void __launch_bounds__(FFT_THREADS)
         __syncthreads();
         len = 8;
     }
+    // the stage records in reverse: tw points just past the last one
     for (lq = (len == 4 ? 0 : 1); len <= P; len <<= 2, lq += 2) {
-        const int q = len >> 2, ts = P / len;
+        const int q = len >> 2;
+        tw -= q;
         for (int t = tid; t < (P >> 2); t += FFT_THREADS) {
             const int j = t & (q - 1), base = ((t >> lq) * len) + j;
+            const double2 w1 = __ldg(&tw[j]), w2 = cmul(w1, w1), w3 = cmul(w2, w1);
             const double2 y0 = fz[fpad(base)];
-            const double2 y2 = cmulc(fz[fpad(base + q)], __ldg(&W[2 * j * ts]));
-            const double2 y1 = cmulc(fz[fpad(base + 2 * q)], __ldg(&W[j * ts]));
-            const double2 y3 = cmulc(fz[fpad(base + 3 * q)], __ldg(&W[3 * j * ts]));
+            const double2 y2 = cmulc(fz[fpad(base + q)], w2);
+            const double2 y1 = cmulc(fz[fpad(base + 2 * q)], w1);
+            const double2 y3 = cmulc(fz[fpad(base + 3 * q)], w3);
             const double2 t0 = cadd(y0, y2), t2 = csub(y0, y2), t1 = cadd(y1, y3);
             const double2 dd = csub(y1, y3);
             const double2 t3 = make_double2(-dd.y, dd.x);  // (y1 - y3) * i
@@ -334,15 +362,36 @@ extern "C" int kk_sirt_update(float* x, const float* g, const float* scale, cons
     return kk_check_launch("kk_sirt_update");
 }
 
-extern "C" int kk_fdk_filter(const kk_projections* src, const double* geom, const double* H, const double* W,
-                             int64_t P, const kk_projections* dst, kk_layered* tex, int64_t layer0, void* stream) {
-    const char* who = "kk_fdk_filter";
-    int rc = check_f32_projections(src, who);
-    if (rc) return rc;
-    if (!H || !W) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: filter or twiddles are NULL", who);
+static int fft_length(int64_t P, const char* who, int* log2P) {
     if (P < 64 || P > FFT_MAX_P || (P & (P - 1)))
         return kk_fail(KK_ERR_UNSUPPORTED, "%s: padded length %lld must be a power of two in [64, %d]", who,
                        (long long)P, FFT_MAX_P);
+    *log2P = 0;
+    while ((1LL << *log2P) < P) ++*log2P;
+    return KK_OK;
+}
+
+extern "C" int64_t kk_fdk_plan_size(int64_t P) { return 3 * P; }
+
+extern "C" int kk_fdk_plan(double* plan, const double* H, int64_t P, void* stream) {
+    const char* who = "kk_fdk_plan";
+    int log2P = 0;
+    int rc = fft_length(P, who, &log2P);
+    if (rc) return rc;
+    if (!plan || !H) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: NULL argument", who);
+    fdk_plan_kernel<<<(unsigned)((P + 255) / 256), 256, 0, (cudaStream_t)stream>>>(plan, H, (int)P, log2P);
+    return kk_check_launch(who);
+}
+
+extern "C" int kk_fdk_filter(const kk_projections* src, const double* geom, const double* plan, int64_t P,
+                             const kk_projections* dst, kk_layered* tex, int64_t layer0, void* stream) {
+    const char* who = "kk_fdk_filter";
+    int rc = check_f32_projections(src, who);
+    if (rc) return rc;
+    if (!plan) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: plan is NULL", who);
+    int log2P = 0;
+    rc = fft_length(P, who, &log2P);
+    if (rc) return rc;
     if (P < 2 * src->cols)
         return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: padded length %lld shorter than 2*cols", who, (long long)P);
     if (dst) {
@@ -360,14 +409,12 @@ extern "C" int kk_fdk_filter(const kk_projections* src, const double* geom, cons
     }
     const int64_t lines = src->n_angles * src->rows;
     if (lines > 0x7ffffffe) return kk_fail(KK_ERR_UNSUPPORTED, "%s: too many rows", who);
-    int log2P = 0;
-    while ((1LL << log2P) < P) ++log2P;
     const size_t smem = sizeof(double2) * (size_t)(P + P / 8);
     rc = kk_allow_smem((const void*)fdk_filter_kernel, smem, who);
     if (rc) return rc;
     fdk_filter_kernel<<<(unsigned)((lines + 1) / 2), FFT_THREADS, smem, (cudaStream_t)stream>>>(
         (const float*)src->data, src->table, src->stride[0], src->stride[1], src->stride[2], (int)lines,
-        (int)src->rows, (int)src->cols, geom, H, (const double2*)W, (int)P, log2P, dst ? (float*)dst->data : nullptr,
+        (int)src->rows, (int)src->cols, geom, plan, (int)P, log2P, dst ? (float*)dst->data : nullptr,
         dst ? dst->table : nullptr, dst ? dst->stride[0] : 0, dst ? dst->stride[1] : 0, dst ? dst->stride[2] : 0,
         tex ? tex->surf : 0, (int)layer0);
     return kk_check_launch(who);

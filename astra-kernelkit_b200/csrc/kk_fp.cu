@@ -2,6 +2,7 @@
 // kk_cone_fp* entry points of include/kk.h.
 #include "kk_async.cuh"
 #include "kk_cone.cuh"
+#include <algorithm>
 #include <climits>
 #include <type_traits>
 
@@ -105,8 +106,8 @@ __device__ __forceinline__ int span_class(float c0, float c1, int n) {
 }
 
 template <typename TV, typename TP, bool TEX8, int EPI, int PATH, int RULE, bool AF = false>
-__device__ __forceinline__ void fp_trace(const FpArgs& L, const kk_fp_angle* P, int a, int A, int D1, int D2, int rule,
-                                         bool a_fast, int r0, int c, int lane) {
+__device__ __forceinline__ void fp_trace(const FpArgs& L, const kk_fp_angle* P, int rec, int a, int A, int D1, int D2,
+                                         int rule, bool a_fast, int r0, int c, int lane) {
     float src[3], cor[3], u[3], v[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -127,6 +128,10 @@ __device__ __forceinline__ void fp_trace(const FpArgs& L, const kk_fp_angle* P, 
         const int64_t off = (int64_t)(r0 + lane + 32 * k) * L.ps[1] + (int64_t)c * L.ps[2];
         return L.table ? (TP*)L.table[a] + off : (TP*)L.out + (int64_t)a * L.ps[0] + off;
     };
+    // running float32 sum of ray k between launches (16-bit outputs)
+    auto sum_ptr = [&](int k) -> float* {
+        return L.sums + ((int64_t)rec * L.rows + (r0 + lane + 32 * k)) * L.cols + c;
+    };
     RaySetup R[FP_RPT];
     float acc[FP_RPT];
 #pragma unroll
@@ -134,7 +139,7 @@ __device__ __forceinline__ void fp_trace(const FpArgs& L, const kk_fp_angle* P, 
         const int r = r0 + lane + 32 * k;
         const bool valid = r < L.rows;
         R[k] = ray_setup(src, cor, u, v, A, D1, D2, valid ? r : 0, c, sc1, sc2);
-        acc[k] = (L.additive && valid) ? ld_rw(out_ptr(k)) : 0.f;
+        acc[k] = !valid ? 0.f : L.load_sums ? *sum_ptr(k) : L.additive ? ld_rw(out_ptr(k)) : 0.f;
     }
 
     const int s_end = min(nS, L.s_end);
@@ -299,6 +304,10 @@ __device__ __forceinline__ void fp_trace(const FpArgs& L, const kk_fp_angle* P, 
 #pragma unroll
     for (int k = 0; k < FP_RPT; ++k) {
         if (r0 + lane + 32 * k >= L.rows) continue;
+        if (L.store_sums) {
+            *sum_ptr(k) = acc[k];
+            continue;
+        }
         float out = acc[k];
         if (EPI == FP_RESIDUAL && L.final_pass) {
             const int r = r0 + lane + 32 * k;
@@ -335,19 +344,19 @@ __device__ __forceinline__ void fp_block(const FpArgs& L, int t) {
     // layered texture is given, so both units share the work
     const bool use_tex = L.vtex && L.rank[A] == 2 && !(__ldg(&P->flags) & KK_FP_NO_TEXTURE);
     if (use_tex && a_fast)
-        fp_trace<TV, TP, TEX8, EPI, 3, 0, true>(L, P, a, A, D1, D2, rule, a_fast, r0, c, lane);
+        fp_trace<TV, TP, TEX8, EPI, 3, 0, true>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
     else if (use_tex)
-        fp_trace<TV, TP, TEX8, EPI, 3, 0, false>(L, P, a, A, D1, D2, rule, a_fast, r0, c, lane);
+        fp_trace<TV, TP, TEX8, EPI, 3, 0, false>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
     else if (shared && rule == 1)
-        fp_trace<TV, TP, TEX8, EPI, 2, 1>(L, P, a, A, D1, D2, rule, a_fast, r0, c, lane);
+        fp_trace<TV, TP, TEX8, EPI, 2, 1>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
     else if (shared)
-        fp_trace<TV, TP, TEX8, EPI, 2, 0>(L, P, a, A, D1, D2, rule, a_fast, r0, c, lane);
+        fp_trace<TV, TP, TEX8, EPI, 2, 0>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
     else if (fast && rule == 1)
-        fp_trace<TV, TP, TEX8, EPI, 1, 1>(L, P, a, A, D1, D2, rule, a_fast, r0, c, lane);
+        fp_trace<TV, TP, TEX8, EPI, 1, 1>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
     else if (fast)
-        fp_trace<TV, TP, TEX8, EPI, 1, 0>(L, P, a, A, D1, D2, rule, a_fast, r0, c, lane);
+        fp_trace<TV, TP, TEX8, EPI, 1, 0>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
     else
-        fp_trace<TV, TP, TEX8, EPI, 0, 0>(L, P, a, A, D1, D2, rule, a_fast, r0, c, lane);
+        fp_trace<TV, TP, TEX8, EPI, 0, 0>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
 }
 
 template <typename TV, typename TP, bool TEX8, int EPI>
@@ -381,7 +390,10 @@ __global__ void __launch_bounds__(32 * FP_COLS, KK_FP_MINBLOCKS) cone_fp_kernel(
 // checked code instead, so the tile path can never read outside a slot.
 constexpr int BRICK_D1 = 10;  // texels of a tile along D1 (one per column, with margins)
 constexpr int BRICK_D2 = 72;  // texels along D2: 288 bytes, a multiple of 16
-constexpr int BRICK_STAGES = 8;
+#ifndef KK_FP_BRICK_STAGES
+#define KK_FP_BRICK_STAGES 8
+#endif
+constexpr int BRICK_STAGES = KK_FP_BRICK_STAGES;
 constexpr int BRICK_TILE_BYTES = BRICK_D1 * BRICK_D2 * 4;
 constexpr int BRICK_STAGE_FLOATS = (BRICK_TILE_BYTES + 127) / 128 * 32;  // 128-byte aligned slots
 constexpr int BRICK_WARPS = FP_COLS + 1;                                   // + the producer
@@ -800,12 +812,51 @@ static bool brick_prepare(FpBrick& B, const FpArgs& L) {
 }
 
 struct FpLaunch {
-    int span_setting;  // as kk_fp_options.span
-    bool tiles;        // shared-memory tiles where the rays qualify
+    int span_setting;    // as kk_fp_options.span
+    bool tiles;          // shared-memory tiles where the rays qualify
+    float* sums;         // float32 running sums for 16-bit outputs, or NULL
+    int64_t sums_elems;  // its size in elements
 };
+
+// 16-bit projections with a float32 running-sum buffer: the records are
+// traced in chunks that fit the buffer, each chunk in span launches whose
+// sums pass through the buffer (the output is written once, by the last
+// launch of the chunk, with the epilogue), so the result is that of one
+// launch bit for bit. The residual may then be computed in place too.
+template <typename TV, typename TP, int EPI>
+static bool launch_fp_sums(const FpArgs& base, bool tex8, cudaStream_t s, const FpLaunch& opt) {
+    const int64_t per = (int64_t)base.rows * base.cols;
+    const int nmax = max(base.vn[0], max(base.vn[1], base.vn[2]));
+    const int span = fp_span(nmax, base.slab, opt.span_setting);
+    if (!opt.sums || opt.sums_elems < per || !span) return false;
+    const int passes = (nmax + span - 1) / span;
+    const int chunk = (int)std::min<int64_t>((int64_t)base.n_angles, opt.sums_elems / per);
+    FpArgs L = base;
+    L.col_tiles = (L.cols + FP_COLS - 1) / FP_COLS;
+    const int row_tiles = (L.rows + FP_ROWS_T - 1) / FP_ROWS_T;
+    L.sums = opt.sums;
+    for (int c0 = 0; c0 < base.n_angles; c0 += chunk) {
+        L.angles = base.angles + c0;
+        L.n_angles = min(chunk, base.n_angles - c0);
+        const int64_t blocks = (int64_t)row_tiles * L.n_angles * L.col_tiles;
+        for (int p = 0; p < passes; ++p) {
+            L.s_begin = p * span;
+            L.s_end = (p + 1) * span;
+            L.load_sums = p > 0;
+            L.store_sums = p < passes - 1;
+            L.final_pass = p == passes - 1;
+            if (tex8)
+                cone_fp_kernel<TV, TP, true, EPI><<<(unsigned)blocks, 32 * FP_COLS, 0, s>>>(L);
+            else
+                cone_fp_kernel<TV, TP, false, EPI><<<(unsigned)blocks, 32 * FP_COLS, 0, s>>>(L);
+        }
+    }
+    return true;
+}
 
 template <typename TV, typename TP, int EPI>
 static void launch_fp_typed(const FpArgs& base, bool tex8, cudaStream_t s, const FpLaunch& opt) {
+    if (!std::is_same<TP, float>::value && launch_fp_sums<TV, TP, EPI>(base, tex8, s, opt)) return;
     FpArgs L = base;
     L.col_tiles = (L.cols + FP_COLS - 1) / FP_COLS;
     const int row_tiles = (L.rows + FP_ROWS_T - 1) / FP_ROWS_T;
@@ -952,7 +1003,9 @@ extern "C" int kk_cone_fp_ex(const kk_volume* vol, const kk_projections* proj, c
         L.vtex = vtex->tex;
     }
     L.additive = opts->additive ? 1 : 0;
-    const FpLaunch lo = {opts->span, (opts->flags & KK_FP_OPT_TILES) != 0};
+    if (opts->sums_elems < 0 || (opts->sums_elems > 0 && !opts->sums))
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: bad running-sum buffer", who);
+    const FpLaunch lo = {opts->span, (opts->flags & KK_FP_OPT_TILES) != 0, opts->sums, opts->sums_elems};
     if (opts->residual) {
         const kk_fp_residual* res = opts->residual;
         if (!res->y || !res->weight) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: residual operands are NULL", who);
@@ -980,9 +1033,12 @@ extern "C" int32_t kk_fp_launches(int32_t max_slices, int32_t slab, int32_t proj
 }
 
 extern "C" int32_t kk_fp_launches_ex(int32_t max_slices, int32_t slab, int32_t proj_dtype, int32_t span) {
+    // launches per chunk of records; 16-bit outputs split only with a
+    // running-sum buffer
     if (max_slices < 1) return 1;
     const int sl = slab > 0 ? slab : FP_SLAB;
-    const int sp = proj_dtype == KK_F32 ? fp_span(max_slices, sl, span) : 0;
+    const int sp = fp_span(max_slices, sl, span);
+    (void)proj_dtype;
     return sp ? (max_slices + sp - 1) / sp : 1;
 }
 

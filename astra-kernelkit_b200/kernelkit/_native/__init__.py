@@ -48,7 +48,8 @@ class kk_fp_options(ctypes.Structure):
     _fields_ = [("interp", ctypes.c_int32), ("slab", ctypes.c_int32),
                 ("additive", ctypes.c_int32), ("span", ctypes.c_int32),
                 ("flags", ctypes.c_int32), ("vtex", ctypes.c_void_p),
-                ("residual", ctypes.c_void_p)]
+                ("residual", ctypes.c_void_p), ("sums", ctypes.c_void_p),
+                ("sums_elems", ctypes.c_int64)]
 
 
 #: kk_fp_options.flags: shared-memory tiles staged by the tensor-copy
@@ -93,7 +94,7 @@ BP_ANGLE_DTYPE = np.dtype([("num_u", "<f4", 4), ("num_v", "<f4", 4),
 
 #: every symbol include/kk.h declares
 EXPORTS = ("kk_cone_fp_ex", "kk_fp_launches_ex", "kk_wait_timeouts",
-           "kk_fdk_filter",
+           "kk_fdk_filter", "kk_fdk_plan", "kk_fdk_plan_size",
            "kk_cone_fp", "kk_cone_fp_residual", "kk_cone_fp_layered",
            "kk_cone_fp_adjoint", "kk_cone_fp_batched",
            "kk_cone_bp_layered_batched",
@@ -153,14 +154,17 @@ def load():
                                             P(kk_bp_update), vp, vp]
     L.kk_preweight.argtypes = [P(kk_projections), vp, vp]
     L.kk_filter_rows.argtypes = [P(kk_projections), vp, i64, vp]
-    L.kk_fdk_filter.argtypes = [P(kk_projections), vp, vp, vp, i64,
+    L.kk_fdk_filter.argtypes = [P(kk_projections), vp, vp, i64,
                                 P(kk_projections), vp, i64, vp]
+    L.kk_fdk_plan.argtypes = [vp, vp, i64, vp]
+    L.kk_fdk_plan_size.argtypes = [i64]
     L.kk_reciprocal.argtypes = [vp, i64, vp]
     L.kk_sirt_update.argtypes = [vp, vp, vp, vp, f32, f32, i32, i32, i64, vp]
     L.kk_fp_set_span.argtypes = [i32]
     L.kk_fp_launches.argtypes = [i32, i32, i32]
     for name in EXPORTS[:-2]:
         getattr(L, name).restype = ctypes.c_int
+    L.kk_fdk_plan_size.restype = ctypes.c_int64
     L.kk_last_error.restype = ctypes.c_char_p
     L.kk_last_error.argtypes = []
     L.kk_abi_version.restype = ctypes.c_int

@@ -170,7 +170,7 @@ def _streamed_bp(projections: np.ndarray, projection_geometry,
             projection_geometry)).cuda()
         P = processing.padded_length(cols)
         if P <= processing.FFT_MAX_P:
-            H, W = processing.device_spectrum(P, filter)
+            plan = processing.device_plan(P, filter)
         else:
             h = processing._device_filter(P, filter)
     if st.get("last") is not None:
@@ -198,7 +198,7 @@ def _streamed_bp(projections: np.ndarray, projection_geometry,
             tex.copy_from(chunk)
             return
         _native.check(L.kk_fdk_filter(
-            d, pw.data_ptr() + a * 13 * 8, H.data_ptr(), W.data_ptr(), P,
+            d, pw.data_ptr() + a * 13 * 8, plan.data_ptr(), P,
             d if in_place else None, tex.handle, 0, stream))
     staged, used = [None, None], [None, None]
     for c, a in enumerate(range(0, n, _CHUNK)):

@@ -125,6 +125,11 @@ class RayDrivenConeFP(BaseKernel):
     #: directly (same results bit for bit; slower at the measured shapes,
     #: so off by default)
     use_tiles = False
+    #: bytes of the float32 buffer that carries the running sums between
+    #: slice-span launches when the projections are 16-bit (angles are
+    #: traced in chunks that fit it); 0 traces 16-bit projections in one
+    #: launch
+    sums_bytes = 1 << 30
 
     def __init__(self, pixels_per_block: tuple = None,
                  slices_per_block: int = None,
@@ -395,8 +400,26 @@ class RayDrivenConeFP(BaseKernel):
         self._launch(vdesc, pdesc, osc, lay, None, additive)
         del keep
 
-    def _options(self, lay, residual, additive) -> "_native.kk_fp_options":
+    def _sums(self, pdesc):
+        """(pointer, elements) of the running-sum buffer for 16-bit
+        projections, allocated once per projector and device."""
+        if pdesc.dtype == _native.KK_F32 or self.sums_bytes <= 0:
+            return None, 0
+        per = int(pdesc.rows) * int(pdesc.cols)
+        n = min(int(pdesc.n_angles), max(1, int(self.sums_bytes) // (4 * per)))
+        t = _arrays.torch()
+        buf = getattr(self, "_sums_buf", None)
+        dev = t.cuda.current_device()
+        if buf is None or buf.numel() < n * per or buf.device.index != dev:
+            buf = t.empty(n * per, dtype=t.float32, device="cuda")
+            self._sums_buf = buf
+        return buf.data_ptr(), buf.numel()
+
+    def _options(self, lay, residual, additive, pdesc=None
+                 ) -> "_native.kk_fp_options":
         o = _native.kk_fp_options()
+        if pdesc is not None:
+            o.sums, o.sums_elems = self._sums(pdesc)
         o.interp = self._interp if lay is None else _native.KK_INTERP_TEX8
         o.slab = self.slices_per_block
         o.additive = int(bool(additive))
@@ -410,7 +433,7 @@ class RayDrivenConeFP(BaseKernel):
         return o
 
     def _launch(self, vdesc, pdesc, osc, lay, residual, additive):
-        o = self._options(lay, residual, additive)
+        o = self._options(lay, residual, additive, pdesc)
         _native.check(_native.load().kk_cone_fp_ex(
             vdesc, pdesc, self._params_dev.data_ptr(), osc.ctypes.data, o,
             _native.current_stream()))
@@ -504,9 +527,13 @@ def set_slices_per_launch(slices: int = 0) -> None:
 
 
 def launches_per_projection(max_slices: int, slab: int = 16,
-                            float32: bool = True, span: int = None) -> int:
+                            float32: bool = True, span: int = None,
+                            sums: bool = False) -> int:
     """Kernel launches of one forward projection of a volume whose longest
-    axis has ``max_slices`` voxels."""
+    axis has ``max_slices`` voxels (16-bit projections: per chunk of
+    angles when a running-sum buffer is used, else one)."""
+    if not float32 and not sums:
+        return 1
     return int(_native.load().kk_fp_launches_ex(
         int(max_slices), int(slab),
         _native.KK_F32 if float32 else _native.KK_F16,

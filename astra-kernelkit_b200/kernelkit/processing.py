@@ -74,17 +74,20 @@ def _device_filter(num, name):
     return _DEVICE_FILTERS[key]
 
 
-def device_spectrum(num, name):
-    """(H, W) on the device for ``kk_fdk_filter``: the frequency response
-    of the filter (float64, length ``num``) and the FFT twiddles
-    exp(-2 pi i k / num) as interleaved float64 pairs."""
-    key = ("spectrum", num, name.lower())
+def device_plan(num, name):
+    """The ``kk_fdk_filter`` plan (device float64) of the filter's
+    frequency response for padded length ``num``."""
+    key = ("plan", num, name.lower())
     if key not in _DEVICE_FILTERS:
         t = _arrays.torch()
-        H = np.ascontiguousarray(_filter(num, name), np.float64)
-        W = np.exp(-2j * np.pi * np.arange(num) / num)
-        W = np.ascontiguousarray(np.stack([W.real, W.imag], axis=1))
-        _DEVICE_FILTERS[key] = (t.from_numpy(H).cuda(), t.from_numpy(W).cuda())
+        L = _native.load()
+        H = t.from_numpy(np.ascontiguousarray(_filter(num, name),
+                                              np.float64)).cuda()
+        plan = t.empty(int(L.kk_fdk_plan_size(num)), dtype=t.float64,
+                       device="cuda")
+        _native.check(L.kk_fdk_plan(plan.data_ptr(), H.data_ptr(), num,
+                                    _native.current_stream()))
+        _DEVICE_FILTERS[key] = plan
     return _DEVICE_FILTERS[key]
 
 
@@ -128,9 +131,9 @@ def filter(projections, verbose: bool = False, filter: str = "ramlak"):
     P = padded_length(int(desc.cols))
     if P <= FFT_MAX_P:
         # float64 FFT filtering in one pass, as the reference (cuFFT)
-        H, W = device_spectrum(P, filter)
+        plan = device_plan(P, filter)
         _native.check(_native.load().kk_fdk_filter(
-            desc, None, H.data_ptr(), W.data_ptr(), P, desc, None, 0,
+            desc, None, plan.data_ptr(), P, desc, None, 0,
             _native.current_stream()))
     else:  # direct circular convolution with the impulse response
         h = _device_filter(P, filter)

@@ -177,6 +177,14 @@ typedef struct {
                                         volume as for kk_cone_fp_layered */
     const kk_fp_residual* residual;  /* NULL, or the SIRT epilogue as for
                                         kk_cone_fp_residual */
+    float* sums;          /* 16-bit projections: float32 device buffer for
+                             the running sums between span launches (the
+                             records are traced in chunks of sums_elems /
+                             (rows * cols) angles); NULL (or too small for
+                             one angle): one launch, as the sums cannot
+                             pass through a 16-bit output unrounded.
+                             Unused for float32 projections */
+    int64_t sums_elems;   /* elements of sums */
 } kk_fp_options;
 
 /* kk_fp_options.flags: rays traced on the CUDA cores sample shared-memory
@@ -206,7 +214,8 @@ KK_API int kk_fp_set_span(int32_t slices);
 
 /* Number of kernel launches kk_cone_fp* makes for a volume whose longest
  * axis has max_slices voxels, with this slab and projection dtype, at the
- * calling thread's span (kk_fp_launches) or a given span (_ex). */
+ * calling thread's span (kk_fp_launches) or a given span (_ex: per chunk
+ * of angles, for any projection dtype given a running-sum buffer). */
 KK_API int32_t kk_fp_launches(int32_t max_slices, int32_t slab,
                               int32_t proj_dtype);
 KK_API int32_t kk_fp_launches_ex(int32_t max_slices, int32_t slab,
@@ -368,18 +377,26 @@ KK_API int kk_filter_rows(const kk_projections* proj, const double* h, int64_t P
  * 96-126, and the copy into the backprojector's texture): every detector
  * row of src is pre-weighted as kk_preweight does (geom as there; NULL
  * skips the weighting), zero-padded to P values, filtered with the
- * frequency response H (P doubles, real and even, as the reference builds
- * it) by a float64 FFT (forward, product, inverse, as the reference does
- * with cuFFT), and its first cols values are stored as float32 into dst
- * (NULL: not stored; dst may be src itself) and into layers [layer0,
- * layer0 + n_angles) of tex (NULL: not stored; a float32 kk_layered of
- * the same rows and cols). W: P complex doubles (re, im) with W[k] =
- * exp(-2 pi i k / P). P is a power of two in [64, 8192], at least 2 cols;
- * float32 data. */
+ * frequency response the plan holds by a float64 FFT (forward, product,
+ * inverse, as the reference does with cuFFT), and its first cols values
+ * are stored as float32 into dst (NULL: not stored; dst may be src
+ * itself) and into layers [layer0, layer0 + n_angles) of tex (NULL: not
+ * stored; a float32 kk_layered of the same rows and cols). P is a power of
+ * two in [64, 8192], at least 2 cols; float32 data. */
 KK_API int kk_fdk_filter(const kk_projections* src, const double* geom,
-                         const double* H, const double* W, int64_t P,
+                         const double* plan, int64_t P,
                          const kk_projections* dst, kk_layered* tex,
                          int64_t layer0, void* stream);
+
+/* The plan kk_fdk_filter reads for padded length P: kk_fdk_plan_size(P)
+ * doubles of device memory (caller-owned), filled on the stream from the
+ * filter's frequency response H (P doubles on the device, real and even,
+ * as processing.py:44-93 builds it): H in bit-reversed order, then for
+ * every radix-4 stage of length len = P, P/4, ... (down to 4) the twiddles
+ * exp(-2 pi i j / len), j < len / 4, as (re, im) pairs. */
+KK_API int64_t kk_fdk_plan_size(int64_t P);
+KK_API int kk_fdk_plan(double* plan, const double* H, int64_t P,
+                       void* stream);
 
 /* ---- elementwise helpers -------------------------------------------- */
 

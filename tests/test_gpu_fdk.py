@@ -22,11 +22,11 @@ def _rows(n, rows, cols, seed):
 
 def _fft_filter(p, name, geom=None, dst=True, tex=None, layer0=0):
     P = processing.padded_length(p.shape[2])
-    H, W = processing.device_spectrum(P, name)
+    plan = processing.device_plan(P, name)
     d = _native.projections_desc(p)
     _native.check(_native.load().kk_fdk_filter(
-        d, None if geom is None else geom.data_ptr(), H.data_ptr(),
-        W.data_ptr(), P, d if dst else None,
+        d, None if geom is None else geom.data_ptr(), plan.data_ptr(),
+        P, d if dst else None,
         None if tex is None else tex.handle, layer0,
         _native.current_stream()))
 
@@ -104,9 +104,30 @@ def test_texture_store_equals_copy(n):
 def test_fdk_filter_rejects_bad_lengths():
     p = _rows(1, 2, 40, 1)
     d = _native.projections_desc(p)
-    H, W = processing.device_spectrum(128, "ramlak")
+    plan = processing.device_plan(128, "ramlak")
     L = _native.load()
     for P in (64, 96, 16384):  # shorter than 2 cols, not a power of two, too long
-        rc = L.kk_fdk_filter(d, None, H.data_ptr(), W.data_ptr(), P, d, None,
-                             0, _native.current_stream())
+        rc = L.kk_fdk_filter(d, None, plan.data_ptr(), P, d, None, 0,
+                             _native.current_stream())
         assert rc != _native.KK_OK
+
+
+@pytest.mark.parametrize("P", [64, 128, 2048, 8192])
+def test_plan_layout(P):
+    """H in bit-reversed order, then per radix-4 stage the twiddles
+    exp(-2 pi i j / len), j < len / 4."""
+    plan = processing.device_plan(P, "cosine").cpu().numpy()
+    H = processing._filter(P, "cosine")
+    L = P.bit_length() - 1
+    rev = [int(format(i, f"0{L}b")[::-1], 2) for i in range(P)]
+    assert np.array_equal(plan[:P], H[rev])
+    off, ln = P, P
+    while ln >= 4:
+        j = np.arange(ln // 4)
+        rec = plan[off:off + 2 * len(j)].reshape(-1, 2)
+        w = np.exp(-2j * np.pi * j / ln)
+        np.testing.assert_allclose(rec[:, 0], w.real, atol=1e-15)
+        np.testing.assert_allclose(rec[:, 1], w.imag, atol=1e-15)
+        off += 2 * len(j)
+        ln //= 4
+    assert off <= 3 * P

@@ -120,3 +120,45 @@ def test_residual_partial_overlap_is_rejected():
     w = torch.ones(shape, device="cuda")
     with pytest.raises(ValueError, match="overlaps"):
         K.residual(vol, pgs, vg, out, y, w)
+
+
+@pytest.mark.parametrize("vdt,half_tex", [(torch.bfloat16, False),
+                                          (torch.bfloat16, True),
+                                          (torch.float32, False)])
+@pytest.mark.parametrize("mode", ["store", "additive", "residual",
+                                  "residual_in_place"])
+def test_16bit_projection_spans_through_the_sums_buffer(vdt, half_tex, mode):
+    """float16 projections traced in 16-slice spans whose float32 running
+    sums pass through the caller's buffer (whole scan, or chunks of 5 and
+    of 1 angles) equal the one-launch result bit for bit."""
+    pgs, vg = build_case("config1")
+    vol = torch.from_numpy(case_volume("config1", vg)).cuda().to(vdt)
+    det = pgs[0].detector
+    shape = (len(pgs), det.rows, det.cols)
+    g = torch.Generator(device="cuda").manual_seed(8)
+    y = torch.rand(shape, generator=g, device="cuda").half()
+    w = torch.rand(shape, generator=g, device="cuda").half()
+    per = det.rows * det.cols * 4
+    outs = []
+    for sums_bytes in (0, 1 << 30, 5 * per, per):
+        K = RayDrivenConeFP()
+        K.half_texture = half_tex
+        K.slices_per_launch = 16
+        K.sums_bytes = sums_bytes
+        K.compile()
+        K.set_params(K.geoms2params(pgs, vg))
+        out = torch.full(shape, 0.25, device="cuda").half()
+        if mode == "store":
+            K(vol, pgs, vg, out, additive=False)
+        elif mode == "additive":
+            K(vol, pgs, vg, out, additive=True)
+        elif mode == "residual":
+            K.residual(vol, pgs, vg, out, y, w)
+        else:
+            out = y.clone()
+            K.residual(vol, pgs, vg, out, out, w)
+        torch.cuda.synchronize()
+        outs.append(out)
+    for o in outs[1:]:
+        assert torch.equal(o, outs[0])
+    assert float(outs[0].float().abs().max()) > 0

@@ -89,7 +89,8 @@ def test_interpolation_mode_checked():
 def test_fp_launch_split_is_host_logic():
     """kk_fp_launches / kk_fp_set_span (no GPU needed): float32 projections
     of volumes longer than 256 slices are traced in 256-slice launches by
-    default; 16-bit projections always in one launch."""
+    default; 16-bit projections in one launch, unless a float32
+    running-sum buffer carries the sums (then per chunk of angles)."""
     from kernelkit.kernels.cone_fp import (launches_per_projection,
                                            set_slices_per_launch)
 
@@ -97,6 +98,9 @@ def test_fp_launch_split_is_host_logic():
     assert launches_per_projection(512) == 2
     assert launches_per_projection(1024) == 4
     assert launches_per_projection(1024, float32=False) == 1
+    assert launches_per_projection(1024, float32=False, sums=True) == 4
+    L = _native.load()
+    assert L.kk_fp_launches(1024, 16, _native.KK_F16) == 1
     try:
         set_slices_per_launch(-1)
         assert launches_per_projection(1024) == 1
