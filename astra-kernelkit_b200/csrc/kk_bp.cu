@@ -1,5 +1,6 @@
 // Cone-beam backprojection (voxel-driven) for sm_100a: kernel, layered
 // projection textures and the kk_cone_bp* entry points of include/kk.h.
+#include <algorithm>
 #include <mutex>
 
 #ifndef KK_BP_LANES
@@ -65,9 +66,9 @@ __device__ __forceinline__ void bp_block(const BpArgs& L, int bx, int by, int bz
         vacc[i] = 0.f;
         if (active && i < cnt) {
             if (L.load_mode == LOAD_VOL)
-                vacc[i] = ld_cs(vol + vbase + i * vstep);
+                vacc[i] = L.fresh ? ld_cv(vol + vbase + i * vstep) : ld_cs(vol + vbase + i * vstep);
             else if (L.load_mode == LOAD_WORK)
-                vacc[i] = ld_cs(L.work + wbase + i * wstep);
+                vacc[i] = L.fresh ? __ldcv(L.work + wbase + i * wstep) : ld_cs(L.work + wbase + i * wstep);
         }
     }
 
@@ -121,7 +122,7 @@ __device__ __forceinline__ void bp_block(const BpArgs& L, int bx, int by, int bz
             st_cs(L.work + wbase + i * wstep, vacc[i]);
         } else if (EPI == BP_UPDATE) {
             const int64_t e = vbase + i * vstep;
-            float x = ld_cs(p);
+            float x = L.fresh ? ld_cv(p) : ld_cs(p);
             x = __fsub_rn(x, __fmul_rn(vacc[i], ld((const TV*)L.upd_scale + e)));
             if (L.upd_mask) x = __fmul_rn(x, ld((const TV*)L.upd_mask + e));
             if (L.has_min) x = fmaxf(x, L.vmin);
@@ -142,8 +143,9 @@ __device__ __forceinline__ void bp_block(const BpArgs& L, int bx, int by, int bz
 // TZ, TY are the largest powers of two up to 8 and 64 dividing the grid's
 // extents nx, ny, so the map from the linear block index is a bijection of
 // the nx x ny x nz grid.
-__device__ __forceinline__ void bp_tile_order(int lin, int nx, int ny, int nz, int& bx, int& by, int& bz) {
-    const int TZ = min(8, nx & -nx), TY = min(64, ny & -ny);
+__device__ __forceinline__ void bp_tile_order(int lin, int nx, int ny, int nz, int& bx, int& by, int& bz,
+                                              int tz_max = 8, int ty_max = 64) {
+    const int TZ = min(tz_max, nx & -nx), TY = min(ty_max, ny & -ny);
     const int per_x = TZ * TY, col_blocks = per_x * nz;
     const int col = lin / col_blocks, r = lin - col * col_blocks;
     bz = r / per_x;
@@ -157,7 +159,7 @@ template <typename TP, typename TV, bool TEX8, int EPI, int FETCH>
 __global__ void __launch_bounds__(BP_TILE_2* BP_TILE_1) cone_bp_kernel(const BpArgs L) {
     int bx, by, bz;
     bp_tile_order(blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z), gridDim.x, gridDim.y,
-                  gridDim.z, bx, by, bz);
+                  gridDim.z, bx, by, bz, L.tile_z > 0 ? L.tile_z : 8, L.tile_y > 0 ? L.tile_y : 64);
     bp_block<TP, TV, TEX8, EPI, FETCH>(L, bx, by, bz);
 }
 
@@ -186,8 +188,108 @@ __global__ void __launch_bounds__(BP_TILE_2* BP_TILE_1) cone_bp_batched_kernel(c
     const int tx = B.tiles[i][0], ty = B.tiles[i][1];
     const int tz = (B.block_start[i + 1] - B.block_start[i]) / (tx * ty);
     int bx, by, bz;
-    bp_tile_order(t, tx, ty, tz, bx, by, bz);
+    bp_tile_order(t, tx, ty, tz, bx, by, bz, Ls.tile_z > 0 ? Ls.tile_z : 8, Ls.tile_y > 0 ? Ls.tile_y : 64);
     bp_block<float, float, true, EPI, FETCH_TEX>(Ls, bx, by, bz);
+}
+
+// ---------------------------------------------------------------------------
+// persistent batched backprojection
+// ---------------------------------------------------------------------------
+// One grid of resident blocks works through every (chunk, problem, tile)
+// item of a batch: a block claims the next item from a counter in global
+// memory, items ordered by chunk index first, so every chunk of a tile is
+// claimed after the tile's previous chunk. An item of chunk c > 0 starts
+// from the running sums its tile's chunk c - 1 left behind: it waits until
+// the tile's counter says c chunks are done (spinning with a clock64()
+// budget; a wait that runs out records a timeout, raises the abort flag
+// and skips the item, and every block stops claiming), runs the same
+// block code as the one-launch-per-chunk path, then publishes c + 1. The
+// item that is waited on was claimed earlier by a running block, which
+// itself only waits on still earlier items, so the waits always end.
+constexpr int BP_MAX_CHUNKS = 64;  // 2048 angles, the layered-texture limit
+
+struct BpSched {
+    int n;       // problems
+    int chunks;  // largest chunk count
+    int items;
+    int skip_item;  // tests of the bounded wait: this item is never run
+    long long budget;
+    int cstart[BP_MAX_CHUNKS + 1];  // first item of each chunk index
+    int nchunks[KK_MAX_BATCH];
+    int tiles[KK_MAX_BATCH];
+    int grid[KK_MAX_BATCH][3];
+    int tile_base[KK_MAX_BATCH];  // first counter of each problem
+    BpArgs p[KK_MAX_BATCH];
+};
+
+static __device__ unsigned int g_bp_timeouts;
+
+__global__ void __launch_bounds__(BP_TILE_2* BP_TILE_1) cone_bp_persistent_kernel(const __grid_constant__ BpSched S,
+                                                                                  int* sync) {
+    __shared__ BpArgs Ls;
+    __shared__ int s_item, s_go;
+    const int tid = threadIdx.y * BP_TILE_2 + threadIdx.x;
+    volatile int* abort_flag = sync + 1;
+    for (;;) {
+        if (tid == 0) s_item = *abort_flag ? S.items : atomicAdd(sync, 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= S.items) return;
+        int c = 0;
+        while (c + 1 < S.chunks && S.cstart[c + 1] <= item) ++c;
+        int t = item - S.cstart[c], p = 0;
+        for (; p + 1 < S.n; ++p) {
+            if (S.nchunks[p] <= c) continue;
+            if (t < S.tiles[p]) break;
+            t -= S.tiles[p];
+        }
+        const int* src = reinterpret_cast<const int*>(&S.p[p]);
+        for (int k = tid; k < (int)(sizeof(BpArgs) / 4); k += BP_TILE_2 * BP_TILE_1)
+            reinterpret_cast<int*>(&Ls)[k] = src[k];
+        volatile int* done = sync + 2 + S.tile_base[p] + t;
+        __syncthreads();
+        if (tid == 0) {
+            bool ok = item != S.skip_item;
+            if (ok && c > 0 && *done < c) {
+                const long long t0 = clock64();
+                while (*done < c) {
+                    if (*abort_flag || clock64() - t0 > S.budget) {
+                        ok = false;
+                        if (!*abort_flag) atomicAdd(&g_bp_timeouts, 1u);
+                        *abort_flag = 1;
+                        break;
+                    }
+                    __nanosleep(256);
+                }
+            }
+            __threadfence();  // the previous chunk's sums before ours
+            Ls.j_begin = c * BP_CHUNK;
+            Ls.j_end = min(Ls.n_angles, Ls.j_begin + BP_CHUNK);
+            const bool update = Ls.upd_scale != nullptr;
+            const bool need_work = S.nchunks[p] > 1 && update;  // float32 volumes
+            const int first_load = (Ls.additive && !update) ? LOAD_VOL : LOAD_ZERO;
+            Ls.load_mode = c == 0 ? first_load : (need_work ? LOAD_WORK : LOAD_VOL);
+            Ls.store_mode = c == S.nchunks[p] - 1 ? STORE_FINAL : (need_work ? STORE_WORK : STORE_VOL);
+            Ls.fresh = 1;
+            s_go = ok;
+        }
+        __syncthreads();
+        if (s_go) {
+            int bx, by, bz;
+            bp_tile_order(t, S.grid[p][0], S.grid[p][1], S.grid[p][2], bx, by, bz, Ls.tile_z > 0 ? Ls.tile_z : 8,
+                          Ls.tile_y > 0 ? Ls.tile_y : 64);
+            if (Ls.upd_scale)
+                bp_block<float, float, true, BP_UPDATE, FETCH_TEX>(Ls, bx, by, bz);
+            else
+                bp_block<float, float, true, BP_STORE, FETCH_TEX>(Ls, bx, by, bz);
+            __syncthreads();
+            if (tid == 0) {
+                __threadfence();  // our sums before the count
+                atomicExch((int*)done, c + 1);
+            }
+        }
+        __syncthreads();  // s_item and Ls are rewritten next round
+    }
 }
 
 }  // namespace kk
@@ -539,13 +641,11 @@ extern "C" int kk_cone_bp_static(const kk_projections* proj, const kk_volume* vo
     return kk_cone_bp(proj, vol, angles, out_scale, interp, additive, scratch, stream);
 }
 
-extern "C" int kk_cone_bp_layered_batched(const kk_bp_problem* pr, int32_t n, void* stream) {
-    const char* who = "kk_cone_bp_layered_batched";
+static int batched_args(const kk_bp_problem* pr, int32_t n, BpArgs* args, int* chunks, int* max_chunks,
+                        const char* who) {
     if (!pr || n < 1 || n > KK_MAX_BATCH)
         return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: need 1..%d problems, got %d", who, KK_MAX_BATCH, n);
-    BpArgs args[KK_MAX_BATCH];
-    int chunks[KK_MAX_BATCH];
-    int max_chunks = 0;
+    *max_chunks = 0;
     for (int i = 0; i < n; ++i) {
         const kk_bp_problem& q = pr[i];
         if (q.vol.dtype != KK_F32) return kk_fail(KK_ERR_UNSUPPORTED, "%s: problem %d: float32 volume only", who, i);
@@ -560,12 +660,102 @@ extern "C" int kk_cone_bp_layered_batched(const kk_bp_problem* pr, int32_t n, vo
         L.has_min = q.update.has_min;
         L.has_max = q.update.has_max;
         L.work = q.work;
+        L.tile_z = q.tile_z;
+        L.tile_y = q.tile_y;
+        if (q.tile_z < 0 || q.tile_y < 0 || (q.tile_z & (q.tile_z - 1)) || (q.tile_y & (q.tile_y - 1)))
+            return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: problem %d: tile shape %d x %d is not a power of two", who,
+                           i, q.tile_z, q.tile_y);
         chunks[i] = (L.n_angles + BP_CHUNK - 1) / BP_CHUNK;
         if (update && chunks[i] > 1 && !q.work)
             return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: problem %d: an update over %d angles needs work", who, i,
                            L.n_angles);
-        max_chunks = max(max_chunks, chunks[i]);
+        *max_chunks = max(*max_chunks, chunks[i]);
     }
+    return KK_OK;
+}
+
+extern "C" int64_t kk_bp_batch_sync_elems(const kk_bp_problem* pr, int32_t n) {
+    if (!pr || n < 1 || n > KK_MAX_BATCH) return -1;
+    int64_t total = 2;
+    for (int i = 0; i < n; ++i) {
+        BpArgs L;
+        if (layered_args(L, pr[i].tex, &pr[i].vol, pr[i].angles, pr[i].out_scale, "kk_bp_batch_sync_elems"))
+            return -1;
+        const dim3 g = bp_grid(L);
+        total += (int64_t)g.x * g.y * g.z;
+    }
+    return total;
+}
+
+extern "C" int kk_cone_bp_layered_batched_ex(const kk_bp_problem* pr, int32_t n, const kk_bp_batch_options* opts,
+                                             void* stream) {
+    const char* who = "kk_cone_bp_layered_batched_ex";
+    if (!opts) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: options are NULL", who);
+    if (!opts->persistent) return kk_cone_bp_layered_batched(pr, n, stream);
+    BpArgs args[KK_MAX_BATCH];
+    int chunks[KK_MAX_BATCH];
+    int max_chunks = 0;
+    int rc = batched_args(pr, n, args, chunks, &max_chunks, who);
+    if (rc) return rc;
+    if (max_chunks > BP_MAX_CHUNKS) return kk_fail(KK_ERR_UNSUPPORTED, "%s: more than %d chunks", who, BP_MAX_CHUNKS);
+    static BpSched S;  // host staging, copied into the launch parameters
+    static std::mutex S_mutex;
+    std::lock_guard<std::mutex> lock(S_mutex);
+    S.n = n;
+    S.chunks = max_chunks;
+    S.skip_item = opts->test_skip_item;
+    S.budget = opts->wait_budget_cycles > 0 ? opts->wait_budget_cycles : (1LL << 31);
+    int64_t counters = 0;
+    for (int i = 0; i < n; ++i) {
+        const dim3 g = bp_grid(args[i]);
+        S.grid[i][0] = (int)g.x;
+        S.grid[i][1] = (int)g.y;
+        S.grid[i][2] = (int)g.z;
+        S.tiles[i] = (int)(g.x * g.y * g.z);
+        S.nchunks[i] = chunks[i];
+        S.tile_base[i] = (int)counters;
+        S.p[i] = args[i];
+        counters += S.tiles[i];
+    }
+    int64_t items = 0;
+    for (int c = 0; c < max_chunks; ++c) {
+        S.cstart[c] = (int)items;
+        for (int i = 0; i < n; ++i)
+            if (chunks[i] > c) items += S.tiles[i];
+    }
+    S.cstart[max_chunks] = (int)items;
+    if (items >= 0x7fffffff) return kk_fail(KK_ERR_UNSUPPORTED, "%s: too many items", who);
+    S.items = (int)items;
+    if (!opts->sync || opts->sync_elems < 2 + counters)
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: sync buffer needs %lld ints", who, (long long)(2 + counters));
+    const cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = cudaMemsetAsync(opts->sync, 0, sizeof(int32_t) * (size_t)(2 + counters), st);
+    if (e != cudaSuccess) return kk_fail(KK_ERR_CUDA, "%s: %s", who, cudaGetErrorString(e));
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cone_bp_persistent_kernel, BP_TILE_2 * BP_TILE_1, 0);
+    if (e != cudaSuccess || per_sm < 1) per_sm = 1;
+    const int64_t grid = std::min<int64_t>(items, (int64_t)per_sm * kk_sm_count());
+    if (grid > 0) {
+        const dim3 block(BP_TILE_2, BP_TILE_1);
+        cone_bp_persistent_kernel<<<(unsigned)grid, block, 0, st>>>(S, opts->sync);
+    }
+    return kk_check_launch(who);
+}
+
+int kk_bp_take_timeouts(unsigned int* n) {
+    unsigned int zero = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(n, g_bp_timeouts, sizeof(*n));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_bp_timeouts, &zero, sizeof(zero));
+    return e == cudaSuccess ? KK_OK : kk_fail(KK_ERR_CUDA, "kk_wait_timeouts: %s", cudaGetErrorString(e));
+}
+
+extern "C" int kk_cone_bp_layered_batched(const kk_bp_problem* pr, int32_t n, void* stream) {
+    const char* who = "kk_cone_bp_layered_batched";
+    BpArgs args[KK_MAX_BATCH];
+    int chunks[KK_MAX_BATCH];
+    int max_chunks = 0;
+    int rc = batched_args(pr, n, args, chunks, &max_chunks, who);
+    if (rc) return rc;
     const cudaStream_t st = (cudaStream_t)stream;
     for (int c = 0; c < max_chunks; ++c) {
         for (int kind = 0; kind < 2; ++kind) {  // plain, then update problems

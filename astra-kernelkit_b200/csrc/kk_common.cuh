@@ -55,6 +55,21 @@ template <typename T>
 __device__ __forceinline__ float ld_cs(const T* p) { return ld_rw(p); }
 template <>
 __device__ __forceinline__ float ld_cs<float>(const float* p) { return __ldcs(p); }
+
+// Load that bypasses the L1 cache: for data other blocks of the same
+// launch may have written since this SM last cached it.
+template <typename T>
+__device__ __forceinline__ float ld_cv(const T* p);
+template <>
+__device__ __forceinline__ float ld_cv<float>(const float* p) { return __ldcv(p); }
+template <>
+__device__ __forceinline__ float ld_cv<__nv_bfloat16>(const __nv_bfloat16* p) {
+    return __bfloat162float(__ushort_as_bfloat16(*(const volatile unsigned short*)p));
+}
+template <>
+__device__ __forceinline__ float ld_cv<__half>(const __half* p) {
+    return __half2float(__ushort_as_half(*(const volatile unsigned short*)p));
+}
 template <typename T>
 __device__ __forceinline__ void st_cs(T* p, float v) { st(p, v); }
 template <>
@@ -242,3 +257,4 @@ int kk_fail(int status, const char* fmt, ...);
 int kk_check_launch(const char* what);
 int kk_allow_smem(const void* kernel, size_t bytes, const char* who);
 int kk_sm_count();
+int kk_bp_take_timeouts(unsigned int* n);

@@ -85,6 +85,9 @@ struct BpArgs {
     int load_mode;            // running sum starts from 0 (LOAD_ZERO), vol, work
     int store_mode;           // partial sum goes to vol (STORE_VOL) or work
     float* work;              // float32 running sums between launches
+    int fresh;                // running sums were written by other blocks of
+                              // this launch: load them past the L1 cache
+    int tile_z, tile_y;       // super-column shape in blocks (0: 8 x 64)
 };
 
 enum BpLoad { LOAD_ZERO = 0, LOAD_VOL = 1, LOAD_WORK = 2 };

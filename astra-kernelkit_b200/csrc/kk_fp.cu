@@ -1044,11 +1044,13 @@ extern "C" int32_t kk_fp_launches_ex(int32_t max_slices, int32_t slab, int32_t p
 
 extern "C" int kk_wait_timeouts(int32_t* count) {
     if (!count) return kk_fail(KK_ERR_INVALID_ARGUMENT, "kk_wait_timeouts: count is NULL");
-    unsigned int n = 0, zero = 0;
+    unsigned int n = 0, zero = 0, nbp = 0;
     cudaError_t e = cudaMemcpyFromSymbol(&n, g_fp_timeouts, sizeof(n));
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_fp_timeouts, &zero, sizeof(zero));
     if (e != cudaSuccess) return kk_fail(KK_ERR_CUDA, "kk_wait_timeouts: %s", cudaGetErrorString(e));
-    *count = (int32_t)n;
+    const int rc = kk_bp_take_timeouts(&nbp);
+    if (rc) return rc;
+    *count = (int32_t)(n + nbp);
     return KK_OK;
 }
 
@@ -1098,59 +1100,84 @@ extern "C" int kk_cone_fp_batched(const kk_fp_problem* pr, int32_t n, int32_t in
     if (!pr || n < 1 || n > KK_MAX_BATCH)
         return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: need 1..%d problems, got %d", who, KK_MAX_BATCH, n);
     const cudaStream_t st = (cudaStream_t)stream;
-    for (int kind = 0; kind < 2; ++kind) {  // plain, then residual problems
-        FpBatch B;  // about 14 KB, copied into the launch's parameters
-        B.n = 0;
-        int64_t total = 0;
-        for (int i = 0; i < n; ++i) {
-            const kk_fp_problem& q = pr[i];
-            const bool res = q.residual.y || q.residual.weight;
-            if (res != (kind == 1)) continue;
-            FpArgs L;
-            int rc = fill_fp_args(L, &q.vol, &q.proj, q.angles, q.out_scale, interp, slab, who);
-            if (rc) return rc;
-            if (q.vol.dtype != KK_F32 || q.proj.dtype != KK_F32)
-                return kk_fail(KK_ERR_UNSUPPORTED, "%s: problem %d: float32 volume and projections only", who, i);
-            if (q.vtex) {
-                int ax_of_rank[3];
-                for (int k = 0; k < 3; ++k) ax_of_rank[L.rank[k]] = k;
-                if (interp != KK_INTERP_TEX8 || q.vtex->dtype != KK_F32 || q.vtex->layers != q.vol.shape[ax_of_rank[2]] ||
-                    q.vtex->height != q.vol.shape[ax_of_rank[1]] || q.vtex->width != q.vol.shape[ax_of_rank[0]])
-                    return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: problem %d: texture does not match the volume", who, i);
-                L.vtex = q.vtex->tex;
-            }
-            if (res) {
-                if (!q.residual.y || !q.residual.weight || q.proj.table)
-                    return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: problem %d: residual needs y, weight, strided data",
-                                   who, i);
-                L.res_y = q.residual.y;
-                L.res_w = q.residual.weight;
-            }
-            L.additive = q.additive ? 1 : 0;
-            L.col_tiles = (L.cols + FP_COLS - 1) / FP_COLS;
-            const int64_t blocks = (int64_t)((L.rows + FP_ROWS_T - 1) / FP_ROWS_T) * L.n_angles * L.col_tiles;
-            B.p[B.n] = L;
-            B.block_start[B.n] = (int)total;
-            total += blocks;
-            ++B.n;
-            if (total >= 0x7fffffffLL) return kk_fail(KK_ERR_UNSUPPORTED, "%s: too many blocks for one launch", who);
-        }
-        if (B.n == 0) continue;
-        B.block_start[B.n] = (int)total;
-        const bool tex8 = interp == KK_INTERP_TEX8;
-        if (kind == 0) {
-            if (tex8)
-                cone_fp_batched_kernel<true, FP_STORE><<<(unsigned)total, 32 * FP_COLS, 0, st>>>(B);
-            else
-                cone_fp_batched_kernel<false, FP_STORE><<<(unsigned)total, 32 * FP_COLS, 0, st>>>(B);
-        } else {
-            if (tex8)
-                cone_fp_batched_kernel<true, FP_RESIDUAL><<<(unsigned)total, 32 * FP_COLS, 0, st>>>(B);
-            else
-                cone_fp_batched_kernel<false, FP_RESIDUAL><<<(unsigned)total, 32 * FP_COLS, 0, st>>>(B);
-        }
-        const int rc = kk_check_launch(who);
+    // every problem's arguments, its slice span and launch count
+    FpArgs args[KK_MAX_BATCH];
+    int spans[KK_MAX_BATCH], passes[KK_MAX_BATCH];
+    int max_passes = 1;
+    for (int i = 0; i < n; ++i) {
+        const kk_fp_problem& q = pr[i];
+        FpArgs& L = args[i];
+        int rc = fill_fp_args(L, &q.vol, &q.proj, q.angles, q.out_scale, interp, slab, who);
         if (rc) return rc;
+        if (q.vol.dtype != KK_F32 || q.proj.dtype != KK_F32)
+            return kk_fail(KK_ERR_UNSUPPORTED, "%s: problem %d: float32 volume and projections only", who, i);
+        if (q.span < -1) return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: problem %d: span %d", who, i, q.span);
+        if (q.vtex) {
+            int ax_of_rank[3];
+            for (int k = 0; k < 3; ++k) ax_of_rank[L.rank[k]] = k;
+            if (interp != KK_INTERP_TEX8 || q.vtex->dtype != KK_F32 || q.vtex->layers != q.vol.shape[ax_of_rank[2]] ||
+                q.vtex->height != q.vol.shape[ax_of_rank[1]] || q.vtex->width != q.vol.shape[ax_of_rank[0]])
+                return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: problem %d: texture does not match the volume", who, i);
+            L.vtex = q.vtex->tex;
+        }
+        const bool res = q.residual.y || q.residual.weight;
+        if (res) {
+            if (!q.residual.y || !q.residual.weight || q.proj.table)
+                return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: problem %d: residual needs y, weight, strided data",
+                               who, i);
+            L.res_y = q.residual.y;
+            L.res_w = q.residual.weight;
+        }
+        L.additive = q.additive ? 1 : 0;
+        L.col_tiles = (L.cols + FP_COLS - 1) / FP_COLS;
+        // a residual computed in place needs its operand intact: one launch
+        const bool in_place = res && (L.res_y == L.out || L.res_w == L.out);
+        const int nmax = max(L.vn[0], max(L.vn[1], L.vn[2]));
+        spans[i] = in_place ? 0 : fp_span(nmax, L.slab, q.span);
+        passes[i] = spans[i] ? (nmax + spans[i] - 1) / spans[i] : 1;
+        max_passes = max(max_passes, passes[i]);
+    }
+    // launch p traces span p of every problem that has one; plain and
+    // residual problems are launched apart
+    for (int p = 0; p < max_passes; ++p) {
+        for (int kind = 0; kind < 2; ++kind) {
+            FpBatch B;  // about 14 KB, copied into the launch's parameters
+            B.n = 0;
+            int64_t total = 0;
+            for (int i = 0; i < n; ++i) {
+                if ((args[i].res_y != nullptr) != (kind == 1) || p >= passes[i]) continue;
+                FpArgs L = args[i];
+                if (spans[i]) {
+                    L.s_begin = p * spans[i];
+                    L.s_end = (p + 1) * spans[i];
+                    L.additive = p == 0 ? args[i].additive : 1;
+                    L.final_pass = p == passes[i] - 1;
+                }
+                const int64_t blocks = (int64_t)((L.rows + FP_ROWS_T - 1) / FP_ROWS_T) * L.n_angles * L.col_tiles;
+                B.p[B.n] = L;
+                B.block_start[B.n] = (int)total;
+                total += blocks;
+                ++B.n;
+                if (total >= 0x7fffffffLL)
+                    return kk_fail(KK_ERR_UNSUPPORTED, "%s: too many blocks for one launch", who);
+            }
+            if (B.n == 0) continue;
+            B.block_start[B.n] = (int)total;
+            const bool tex8 = interp == KK_INTERP_TEX8;
+            if (kind == 0) {
+                if (tex8)
+                    cone_fp_batched_kernel<true, FP_STORE><<<(unsigned)total, 32 * FP_COLS, 0, st>>>(B);
+                else
+                    cone_fp_batched_kernel<false, FP_STORE><<<(unsigned)total, 32 * FP_COLS, 0, st>>>(B);
+            } else {
+                if (tex8)
+                    cone_fp_batched_kernel<true, FP_RESIDUAL><<<(unsigned)total, 32 * FP_COLS, 0, st>>>(B);
+                else
+                    cone_fp_batched_kernel<false, FP_RESIDUAL><<<(unsigned)total, 32 * FP_COLS, 0, st>>>(B);
+            }
+            const int rc = kk_check_launch(who);
+            if (rc) return rc;
+        }
     }
     return KK_OK;
 }

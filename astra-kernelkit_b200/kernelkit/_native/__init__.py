@@ -71,14 +71,23 @@ class kk_fp_problem(ctypes.Structure):
     _fields_ = [("vol", kk_volume), ("proj", kk_projections),
                 ("angles", ctypes.c_void_p),
                 ("out_scale", ctypes.c_float * 9), ("vtex", ctypes.c_void_p),
-                ("residual", kk_fp_residual), ("additive", ctypes.c_int32)]
+                ("residual", kk_fp_residual), ("additive", ctypes.c_int32),
+                ("span", ctypes.c_int32)]
 
 
 class kk_bp_problem(ctypes.Structure):
     _fields_ = [("tex", ctypes.c_void_p), ("vol", kk_volume),
                 ("angles", ctypes.c_void_p), ("out_scale", ctypes.c_float),
                 ("update", kk_bp_update), ("work", ctypes.c_void_p),
-                ("additive", ctypes.c_int32)]
+                ("additive", ctypes.c_int32), ("tile_z", ctypes.c_int32),
+                ("tile_y", ctypes.c_int32)]
+
+
+class kk_bp_batch_options(ctypes.Structure):
+    _fields_ = [("persistent", ctypes.c_int32), ("sync", ctypes.c_void_p),
+                ("sync_elems", ctypes.c_int64),
+                ("wait_budget_cycles", ctypes.c_int64),
+                ("test_skip_item", ctypes.c_int32)]
 
 
 #: kk_fp_angle as a NumPy record (64 bytes)
@@ -95,6 +104,7 @@ BP_ANGLE_DTYPE = np.dtype([("num_u", "<f4", 4), ("num_v", "<f4", 4),
 #: every symbol include/kk.h declares
 EXPORTS = ("kk_cone_fp_ex", "kk_fp_launches_ex", "kk_wait_timeouts",
            "kk_fdk_filter", "kk_fdk_plan", "kk_fdk_plan_size",
+           "kk_cone_bp_layered_batched_ex", "kk_bp_batch_sync_elems",
            "kk_cone_fp", "kk_cone_fp_residual", "kk_cone_fp_layered",
            "kk_cone_fp_adjoint", "kk_cone_fp_batched",
            "kk_cone_bp_layered_batched",
@@ -140,6 +150,9 @@ def load():
                                      vp, i32, i32, i32, vp, i64, vp]
     L.kk_cone_fp_batched.argtypes = [P(kk_fp_problem), i32, i32, i32, vp]
     L.kk_cone_bp_layered_batched.argtypes = [P(kk_bp_problem), i32, vp]
+    L.kk_cone_bp_layered_batched_ex.argtypes = [P(kk_bp_problem), i32,
+                                                P(kk_bp_batch_options), vp]
+    L.kk_bp_batch_sync_elems.argtypes = [P(kk_bp_problem), i32]
     L.kk_cone_bp.argtypes = [P(kk_projections), P(kk_volume), vp, f32, i32,
                              i32, vp, vp]
     L.kk_cone_bp_update.argtypes = [P(kk_projections), P(kk_volume), vp, f32,
@@ -165,6 +178,7 @@ def load():
     for name in EXPORTS[:-2]:
         getattr(L, name).restype = ctypes.c_int
     L.kk_fdk_plan_size.restype = ctypes.c_int64
+    L.kk_bp_batch_sync_elems.restype = ctypes.c_int64
     L.kk_last_error.restype = ctypes.c_char_p
     L.kk_last_error.argtypes = []
     L.kk_abi_version.restype = ctypes.c_int

@@ -4,9 +4,13 @@ Volumes and scans of different sizes (e.g. a stack of small samples) are
 solved together: every SIRT iteration of every problem is one batched
 forward-projection launch (``kk_cone_fp_batched``: up to 64 problems per
 launch, each thread block picking its own problem), the texture refills,
-and one batched backprojection launch per 32-angle chunk index
-(``kk_cone_bp_layered_batched``). The whole iteration sequence can be
-captured in one CUDA graph. Launch-shape choices are made per problem
+and one persistent backprojection launch (``kk_cone_bp_layered_batched_ex``:
+resident thread blocks claim (chunk, problem, tile) items in chunk order,
+each waiting with a bounded spin for its tile's previous chunk) or, with
+``persistent=False``, one launch per 32-angle chunk index. The whole
+iteration sequence can be captured in one CUDA graph. Launch-shape
+choices (the forward projector's record grouping, the backprojection's
+super-column shape, the slice span per launch) are made per problem
 shape by ``Autotuner`` (timed on the problems themselves, cached).
 
 This has no counterpart in the reference, which solves one problem per
@@ -72,6 +76,13 @@ class Autotuner:
 #: of one ray axis are launched back to back)
 AXIS_GROUPS = (1, 2, 4, 8)
 
+#: backprojection super-column shapes tried (thread blocks along the
+#: fastest x middle volume axes swept together along the slowest)
+BP_TILES = ((8, 64), (4, 32), (8, 16), (2, 8))
+
+#: forward-projection slice spans tried (slices per launch; 0 = 256)
+FP_SPANS = (0, 96, 64)
+
 
 class BatchedSIRT:
     """SIRT on many problems at once.
@@ -85,10 +96,11 @@ class BatchedSIRT:
 
     def __init__(self, problems, mask=None, min_constraint: float = None,
                  max_constraint: float = None,
-                 autotuner: Autotuner | None = None):
+                 autotuner: Autotuner | None = None, persistent: bool = True):
         t = _arrays.torch()
         self.solvers = []
         self._vtex = []
+        self.persistent = bool(persistent)
         for i, (y, pg, vg) in enumerate(problems):
             s = SIRT(y, pg, vg, mask=None if mask is None else mask[i],
                      min_constraint=min_constraint,
@@ -111,42 +123,78 @@ class BatchedSIRT:
                 _native.volume_desc(s.x), _native.projections_desc(s.y_tmp),
                 s.fp._params_dev.data_ptr(),
                 (ctypes_float9(osc)), lay.handle if lay is not None else None,
-                _native.kk_fp_residual(s.y.data_ptr(), s.R.data_ptr()), 0))
+                _native.kk_fp_residual(s.y.data_ptr(), s.R.data_ptr()), 0,
+                int(getattr(s, "_fp_span", 0))))
             upd = _native.kk_bp_update(
                 s.C.data_ptr(), _native.ptr(s.mask),
                 float(s.min_c) if s.min_c is not None else 0.0,
                 float(s.max_c) if s.max_c is not None else 0.0,
                 int(s.min_c is not None), int(s.max_c is not None))
+            tz, ty = getattr(s, "_bp_tile", (0, 0))
             self._bp.append(_native.kk_bp_problem(
                 s.tex.handle, _native.volume_desc(s.x),
                 s.bp._params_dev.data_ptr(),
                 float(np.float32(s.vg.voxel_volume())), upd,
-                s.bp._work_for(s.x, True) or None, 0))
+                s.bp._work_for(s.x, True) or None, 0, tz, ty))
         n = len(self.solvers)
         self._fp_groups = []
         self._bp_groups = []
+        L = _native.load()
         for g in range(0, n, _native.KK_MAX_BATCH):
             m = min(_native.KK_MAX_BATCH, n - g)
             fa = (_native.kk_fp_problem * m)(*self._fp[g:g + m])
             ba = (_native.kk_bp_problem * m)(*self._bp[g:g + m])
+            opts = None
+            if self.persistent:
+                elems = int(L.kk_bp_batch_sync_elems(ba, m))
+                if elems < 0:
+                    _native.check(_native.KK_ERR_INVALID_ARGUMENT)
+                sync = t.zeros(elems, dtype=t.int32, device="cuda")
+                opts = _native.kk_bp_batch_options(1, sync.data_ptr(), elems,
+                                                   0, -1)
+                opts._sync = sync  # keep the buffer alive with the options
             self._fp_groups.append((fa, m))
-            self._bp_groups.append((ba, m))
+            self._bp_groups.append((ba, m, opts))
         self._graph = None
         self._t = t
 
     @staticmethod
     def _tune(s: SIRT, tuner: Autotuner):
-        key = "fp_axis_group:" + json.dumps(
-            [list(s.x.shape), int(s.y.shape[0]), list(s.y.shape[1:])])
+        sig = json.dumps([list(s.x.shape), int(s.y.shape[0]),
+                          list(s.y.shape[1:])])
 
         def run(g):
             s.fp.axis_group = int(g)
             s.fp._upload()
             s.fp.residual(s.x, s.pg, s.vg, s.y_tmp, s.y, s.R)
 
-        best = tuner.pick(key, AXIS_GROUPS, run)
+        best = tuner.pick("fp_axis_group:" + sig, AXIS_GROUPS, run)
         s.fp.axis_group = int(best)
         s.fp._upload()
+
+        def run_span(span):
+            s.fp.slices_per_launch = int(span)
+            s.fp.residual(s.x, s.pg, s.vg, s.y_tmp, s.y, s.R)
+
+        s._fp_span = int(tuner.pick("fp_span:" + sig, FP_SPANS, run_span))
+        s.fp.slices_per_launch = s._fp_span
+        # backprojection block order: a plain backprojection of the
+        # problem's texture into a scratch volume per candidate shape
+        scratch = _arrays.torch().empty_like(s.x)
+        L = _native.load()
+        zero = _native.kk_bp_update(None, None, 0.0, 0.0, 0, 0)
+
+        def run_bp(shape):
+            one = (_native.kk_bp_problem * 1)(_native.kk_bp_problem(
+                s.tex.handle, _native.volume_desc(scratch),
+                s.bp._params_dev.data_ptr(),
+                float(np.float32(s.vg.voxel_volume())), zero, None, 0,
+                int(shape[0]), int(shape[1])))
+            _native.check(L.kk_cone_bp_layered_batched(
+                one, 1, _native.current_stream()))
+
+        s._bp_tile = tuple(tuner.pick("bp_tile:" + sig, BP_TILES, run_bp))
+        del scratch
 
     @property
     def volumes(self):
@@ -167,8 +215,12 @@ class BatchedSIRT:
                 fa, m, _native.KK_INTERP_TEX8, 16, stream))
         for s in self.solvers:
             s.tex.copy_from(s.y_tmp)
-        for ba, m in self._bp_groups:
-            _native.check(L.kk_cone_bp_layered_batched(ba, m, stream))
+        for ba, m, opts in self._bp_groups:
+            if opts is None:
+                _native.check(L.kk_cone_bp_layered_batched(ba, m, stream))
+            else:
+                _native.check(L.kk_cone_bp_layered_batched_ex(ba, m, opts,
+                                                              stream))
 
     def capture(self, iters: int = 1):
         """Capture ``iters`` iterations into one CUDA graph."""
@@ -203,4 +255,4 @@ def ctypes_float9(a) -> object:
     return (ctypes.c_float * 9)(*[float(v) for v in np.asarray(a).reshape(9)])
 
 
-__all__ = ["Autotuner", "BatchedSIRT", "AXIS_GROUPS"]
+__all__ = ["Autotuner", "BatchedSIRT", "AXIS_GROUPS", "BP_TILES", "FP_SPANS"]

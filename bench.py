@@ -383,26 +383,60 @@ def run_sirt(workload="config2", iters=50):
     scale = float((rec * truth).sum() / (rec * rec).sum())
     fdk_fit = rel(scale * rec)
     del rec
-    solver = SIRT(y, pgs, vg)
-    solver.capture()
-    torch.cuda.synchronize()
-    a = torch.cuda.Event(enable_timing=True)
-    b = torch.cuda.Event(enable_timing=True)
-    a.record()
-    solver.run(iters, use_graph=True)
-    b.record()
-    torch.cuda.synchronize()
-    ms = a.elapsed_time(b)
+    # the reconstructions' projections against exact FP64 line integrals
+    # of the phantom on 16 evenly spaced angles
+    from kernelkit.kernels import RayDrivenConeFP
+
+    sel = list(range(0, len(pgs), len(pgs) // 16))[:16]
+    ssrc, spix = phantom.pixel_centres([pgs[i] for i in sel])
+    exact = phantom.line_integrals(ell, ssrc, spix, device="cuda")
+    fsub = RayDrivenConeFP()
+    fsub.compile()
+    fsub.set_params(fsub.geoms2params([pgs[i] for i in sel], vg))
+
+    def proj_err(x):
+        sub = torch.empty(exact.shape, device="cuda")
+        fsub(x.float(), [pgs[i] for i in sel], vg, sub, additive=False)
+        return float((sub.double() - exact).norm() / exact.norm())
+
     out = {"workload": workload, "iters": iters,
-           "it_per_s": iters / (ms * 1e-3), "ms_per_iter": ms / iters,
-           "dtype": "f32", "rel_l2_phantom": rel(solver.x),
+           "noise": "Poisson, 1e4 photons, log transformed",
            "fdk_rel_l2_phantom": fdk_raw,
            "fdk_rel_l2_phantom_scaled": fdk_fit,
-           "noise": "Poisson, 1e4 photons, log transformed",
            "timing": "CUDA events around the graph replays (FP with "
                      "residual epilogue, texture refill, BP with update "
                      "epilogue per iteration)"}
-    del solver
+    xs = {}
+    for name, vdt, pdt in (("f32", None, None),
+                           ("bf16_volume_f16_projections", torch.bfloat16,
+                            torch.float16)):
+        solver = SIRT(y, pgs, vg, volume_dtype=vdt, projection_dtype=pdt)
+        solver.capture()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        solver.run(iters, use_graph=True)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        xs[name] = solver.x.float().clone()
+        out[name] = {"it_per_s": iters / (ms * 1e-3), "ms_per_iter": ms / iters,
+                     "rel_l2_phantom": rel(xs[name]),
+                     "rel_l2_projections_vs_fp64_16_angles":
+                         proj_err(xs[name])}
+        del solver
+        torch.cuda.empty_cache()
+    h = out["bf16_volume_f16_projections"]
+    h["rel_l2_to_f32_reconstruction"] = float(
+        (xs["bf16_volume_f16_projections"] - xs["f32"]).norm()
+        / xs["f32"].norm())
+    out["speedup_16bit_over_f32"] = h["it_per_s"] / out["f32"]["it_per_s"]
+    # the f32 figures at the top level as before
+    out.update(it_per_s=out["f32"]["it_per_s"],
+               ms_per_iter=out["f32"]["ms_per_iter"], dtype="f32",
+               rel_l2_phantom=out["f32"]["rel_l2_phantom"])
+    del xs, exact
     torch.cuda.empty_cache()
     return out
 

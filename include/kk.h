@@ -223,8 +223,9 @@ KK_API int32_t kk_fp_launches_ex(int32_t max_slices, int32_t slab,
 
 /* Number of waits inside the library's kernels on the current device that
  * gave up since the previous call (and resets it): the shared-memory tile
- * pipeline bounds every wait on a copy or a slot (about a second) and a
- * kernel whose wait runs out stops and leaves its outputs unwritten
+ * pipeline of the forward projection and the persistent batched
+ * backprojection bound every wait (on a copy, a slot or a previous chunk)
+ * and a kernel whose wait runs out stops and leaves its outputs unwritten
  * instead of hanging. 0 in normal operation. Synchronous. */
 KK_API int kk_wait_timeouts(int32_t* count);
 
@@ -329,11 +330,14 @@ typedef struct {
                                    or NULL */
     kk_fp_residual residual;    /* y and weight NULL: plain projection */
     int32_t additive;
+    int32_t span;               /* slices per launch, as kk_fp_options.span
+                                   (0: 256, -1: one launch) */
 } kk_fp_problem;
 
 /* kk_cone_fp / kk_cone_fp_layered / kk_cone_fp_residual for n problems
- * (1 <= n <= KK_MAX_BATCH) in at most two launches (plain and residual
- * problems are launched apart). Results equal the one-problem calls. */
+ * (1 <= n <= KK_MAX_BATCH): launch k traces slice span k of every problem
+ * that has one, plain and residual problems launched apart. Results equal
+ * the one-problem calls. */
 KK_API int kk_cone_fp_batched(const kk_fp_problem* problems, int32_t n,
                               int32_t interp, int32_t slab, void* stream);
 
@@ -347,6 +351,10 @@ typedef struct {
                                    required for an update over more than
                                    32 angles */
     int32_t additive;
+    int32_t tile_z, tile_y;     /* block order: super-columns of tile_z x
+                                   tile_y thread blocks of the two faster
+                                   volume axes (powers of two; 0: 8 x 64),
+                                   a shape the autotuner may choose */
 } kk_bp_problem;
 
 /* kk_cone_bp_layered / kk_cone_bp_layered_update for n problems: one
@@ -355,6 +363,36 @@ typedef struct {
  * the one-problem calls. */
 KK_API int kk_cone_bp_layered_batched(const kk_bp_problem* problems, int32_t n,
                                       void* stream);
+
+typedef struct {
+    int32_t persistent;         /* 0: as kk_cone_bp_layered_batched */
+    int32_t* sync;              /* device ints for the persistent launch's
+                                   work counter, abort flag and per-tile
+                                   chunk counters: kk_bp_batch_sync_elems;
+                                   zeroed by the call (on the stream) */
+    int64_t sync_elems;
+    int64_t wait_budget_cycles; /* bound of a wait on the previous chunk
+                                   of a tile, in SM clocks (0: 2^31, about
+                                   a second) */
+    int32_t test_skip_item;     /* -1; for tests of the bounded wait: the
+                                   item with this index is never run, so
+                                   the tile's next chunk waits out the
+                                   budget, the launch aborts and
+                                   kk_wait_timeouts reports it */
+} kk_bp_batch_options;
+
+/* The batched backprojection as ONE persistent launch (no counterpart in
+ * the reference): resident thread blocks claim (chunk, problem, tile)
+ * items, chunk index first, from a counter; an item of chunk c of a tile
+ * waits (bounded) for the tile's chunk c - 1, then adds its 32 angles to
+ * the running sums with the same block code, so results equal
+ * kk_cone_bp_layered_batched bit for bit. Float32 volumes. */
+KK_API int kk_cone_bp_layered_batched_ex(const kk_bp_problem* problems,
+                                         int32_t n,
+                                         const kk_bp_batch_options* opts,
+                                         void* stream);
+KK_API int64_t kk_bp_batch_sync_elems(const kk_bp_problem* problems,
+                                      int32_t n);
 
 /* ---- FDK pre-processing ---------------------------------------------- */
 

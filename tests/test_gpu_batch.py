@@ -13,7 +13,7 @@ import kernelkit as kk
 from conftest import rel_l2
 from helpers import build_case, case_volume
 from kernelkit import _native
-from kernelkit.batch import Autotuner, BatchedSIRT
+from kernelkit.batch import BP_TILES, FP_SPANS, Autotuner, BatchedSIRT
 from kernelkit.kernels import RayDrivenConeFP, VoxelDrivenConeBP
 
 pytestmark = pytest.mark.gpu
@@ -135,12 +135,147 @@ def test_autotuner_picks_and_caches(tmp_path):
     path = tmp_path / "tune.json"
     tuner = Autotuner(str(path), reps=1)
     b = BatchedSIRT(probs, autotuner=tuner)
-    assert len(tuner.cache) == 2
-    assert all(v in (1, 2, 4, 8) for v in tuner.cache.values())
-    assert [s.fp.axis_group for s in b.solvers] == list(tuner.cache.values())
+    fp_keys = [k for k in tuner.cache if k.startswith("fp_axis_group:")]
+    bp_keys = [k for k in tuner.cache if k.startswith("bp_tile:")]
+    span_keys = [k for k in tuner.cache if k.startswith("fp_span:")]
+    assert len(fp_keys) == 2 and len(bp_keys) == 2 and len(span_keys) == 2
+    assert all(tuner.cache[k] in FP_SPANS for k in span_keys)
+    assert all(tuner.cache[k] in (1, 2, 4, 8) for k in fp_keys)
+    assert all(tuple(tuner.cache[k]) in BP_TILES for k in bp_keys)
+    assert [s.fp.axis_group for s in b.solvers] == [tuner.cache[k]
+                                                    for k in fp_keys]
+    assert [s._bp_tile for s in b.solvers] == [tuple(tuner.cache[k])
+                                               for k in bp_keys]
     # a second tuner reads the file and times nothing
     again = Autotuner(str(path))
     calls = []
-    assert again.pick(next(iter(tuner.cache)), (1, 2),
+    assert again.pick(fp_keys[0], (1, 2),
                       lambda c: calls.append(c)) in (1, 2, 4, 8)
     assert calls == []
+
+
+def _bp_batch(cases, update=False):
+    """kk_bp_problem array over random sinograms of the golden cases (with
+    the SIRT update epilogue when ``update``), fresh volumes, keep-alive."""
+    arr = (_native.kk_bp_problem * len(cases))()
+    outs, keep = [], []
+    for i, case in enumerate(cases):
+        pgs, vg = build_case(case)
+        det = pgs[0].detector
+        g = torch.Generator(device="cuda").manual_seed(20 + i)
+        y = torch.rand((len(pgs), det.rows, det.cols), generator=g,
+                       device="cuda")
+        bp = VoxelDrivenConeBP()
+        bp.compile()
+        bp.set_params(bp.geoms2params(pgs, vg))
+        lay = _native.Layered(*y.shape, _native.KK_F32)
+        lay.copy_from(y)
+        shape = tuple(int(s) for s in vg.shape)
+        out = torch.rand(shape, generator=g, device="cuda")
+        scale = torch.rand(shape, generator=g, device="cuda")
+        work = torch.empty(out.numel(), device="cuda")
+        upd = (_native.kk_bp_update(scale.data_ptr(), None, 0.0, 0.0, 1, 0)
+               if update else _native.kk_bp_update(None, None, 0.0, 0.0, 0, 0))
+        arr[i] = _native.kk_bp_problem(
+            lay.handle, _native.volume_desc(out), bp._params_dev.data_ptr(),
+            float(np.float32(vg.voxel_volume())), upd,
+            work.data_ptr() if update else None, 0, 2 * (i % 2), 0)
+        keep += [lay, bp, y, scale, work]
+        outs.append(out)
+    return arr, outs, keep
+
+
+@pytest.mark.parametrize("update", [False, True])
+def test_persistent_backprojection_equals_per_chunk_launches(update):
+    """One persistent launch walking (chunk, problem, tile) items gives the
+    per-chunk-index launches' volumes bit for bit (96-, 24-, 18- and
+    12-angle scans: 3, 1, 1 and 1 chunks)."""
+    cases = ("config1", "small", "alldirs", "volrot")
+    arr, ref, keep = _bp_batch(cases, update)
+    start = [o.clone() for o in ref]
+    _native.check(_native.load().kk_cone_bp_layered_batched(
+        arr, len(cases), _native.current_stream()))
+    arr2, got, keep2 = _bp_batch(cases, update)
+    for g, s0 in zip(got, start):
+        g.copy_(s0)
+    L = _native.load()
+    elems = int(L.kk_bp_batch_sync_elems(arr2, len(cases)))
+    sync = torch.zeros(elems, dtype=torch.int32, device="cuda")
+    opts = _native.kk_bp_batch_options(1, sync.data_ptr(), elems, 0, -1)
+    for _ in range(2):  # the counters are re-zeroed by every call
+        for g, s0 in zip(got, start):
+            g.copy_(s0)
+        _native.check(L.kk_cone_bp_layered_batched_ex(
+            arr2, len(cases), opts, _native.current_stream()))
+        torch.cuda.synchronize()
+        for a, b in zip(got, ref):
+            assert torch.equal(a, b)
+    assert _native.wait_timeouts() == 0
+
+
+def test_persistent_backprojection_wait_runs_out():
+    """An item that never completes (a flag nothing sets): the item of the
+    tile's next chunk waits out a short budget, the launch aborts instead
+    of hanging and the host reads the timeout; the library keeps working."""
+    cases = ("config1", "small")
+    arr, outs, keep = _bp_batch(cases)
+    L = _native.load()
+    elems = int(L.kk_bp_batch_sync_elems(arr, len(cases)))
+    sync = torch.zeros(elems, dtype=torch.int32, device="cuda")
+    assert _native.wait_timeouts() == 0
+    opts = _native.kk_bp_batch_options(1, sync.data_ptr(), elems, 1 << 20, 0)
+    _native.check(L.kk_cone_bp_layered_batched_ex(
+        arr, len(cases), opts, _native.current_stream()))
+    torch.cuda.synchronize()
+    assert _native.wait_timeouts() >= 1
+    assert int(sync[1]) == 1  # the abort flag
+    # a normal call afterwards completes without timeouts
+    opts.test_skip_item = -1
+    _native.check(L.kk_cone_bp_layered_batched_ex(
+        arr, len(cases), opts, _native.current_stream()))
+    torch.cuda.synchronize()
+    assert _native.wait_timeouts() == 0
+    assert int(sync[0]) >= 1
+
+
+def test_batched_forward_projection_spans_per_problem():
+    """Problems traced in slice spans of their own (16, 48, one launch)
+    within the batched launches give their one-launch results bit for
+    bit."""
+    probs = [_problem(c) for c in CASES]
+    arr = (_native.kk_fp_problem * len(probs))()
+    refs, keep = [], []
+    for i, (pgs, vg, vol, fp, proj) in enumerate(probs):
+        vdesc = _native.volume_desc(vol)
+        osc = np.asarray(fp._output_scale(vg.voxel_size), np.float32)
+        arr[i] = _native.kk_fp_problem(
+            vdesc, _native.projections_desc(proj), fp._params_dev.data_ptr(),
+            (ctypes.c_float * 9)(*osc.reshape(9).tolist()), None,
+            _native.kk_fp_residual(None, None), 1, -1)
+    L = _native.load()
+    for _, _, _, _, proj in probs:
+        proj.fill_(0.5)
+    _native.check(L.kk_cone_fp_batched(arr, len(probs),
+                                       _native.KK_INTERP_TEX8, 16,
+                                       _native.current_stream()))
+    refs = [p[4].clone() for p in probs]
+    for i, span in enumerate((16, 48, -1, 16)):
+        arr[i].span = span
+    for _, _, _, _, proj in probs:
+        proj.fill_(0.5)
+    _native.check(L.kk_cone_fp_batched(arr, len(probs),
+                                       _native.KK_INTERP_TEX8, 16,
+                                       _native.current_stream()))
+    torch.cuda.synchronize()
+    for (_, _, _, _, proj), ref in zip(probs, refs):
+        assert torch.equal(proj, ref)
+
+
+def test_batched_sirt_persistent_equals_per_chunk():
+    probs = _sirt_problems()
+    a = BatchedSIRT(probs, min_constraint=0.0, persistent=True)
+    b = BatchedSIRT(probs, min_constraint=0.0, persistent=False)
+    xa = [x.clone() for x in a.run(3, use_graph=True)]
+    xb = b.run(3, use_graph=True)
+    for u, v in zip(xa, xb):
+        assert torch.equal(u, v)
