@@ -105,7 +105,7 @@ __device__ __forceinline__ int span_class(float c0, float c1, int n) {
     return 1;
 }
 
-template <typename TV, typename TP, bool TEX8, int EPI, int PATH, int RULE, bool AF = false>
+template <typename TV, typename TP, bool TEX8, int EPI, int PATH, int RULE, bool AF = false, bool SUMS = false>
 __device__ __forceinline__ void fp_trace(const FpArgs& L, const kk_fp_angle* P, int rec, int a, int A, int D1, int D2,
                                          int rule, bool a_fast, int r0, int c, int lane) {
     float src[3], cor[3], u[3], v[3];
@@ -139,7 +139,7 @@ __device__ __forceinline__ void fp_trace(const FpArgs& L, const kk_fp_angle* P, 
         const int r = r0 + lane + 32 * k;
         const bool valid = r < L.rows;
         R[k] = ray_setup(src, cor, u, v, A, D1, D2, valid ? r : 0, c, sc1, sc2);
-        acc[k] = !valid ? 0.f : L.load_sums ? *sum_ptr(k) : L.additive ? ld_rw(out_ptr(k)) : 0.f;
+        acc[k] = !valid ? 0.f : (SUMS && L.load_sums) ? *sum_ptr(k) : L.additive ? ld_rw(out_ptr(k)) : 0.f;
     }
 
     const int s_end = min(nS, L.s_end);
@@ -304,7 +304,7 @@ __device__ __forceinline__ void fp_trace(const FpArgs& L, const kk_fp_angle* P, 
 #pragma unroll
     for (int k = 0; k < FP_RPT; ++k) {
         if (r0 + lane + 32 * k >= L.rows) continue;
-        if (L.store_sums) {
+        if (SUMS && L.store_sums) {
             *sum_ptr(k) = acc[k];
             continue;
         }
@@ -318,7 +318,7 @@ __device__ __forceinline__ void fp_trace(const FpArgs& L, const kk_fp_angle* P, 
     }
 }
 
-template <typename TV, typename TP, bool TEX8, int EPI>
+template <typename TV, typename TP, bool TEX8, int EPI, bool SUMS = false>
 __device__ __forceinline__ void fp_block(const FpArgs& L, int t) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int ct = t % L.col_tiles;
@@ -344,24 +344,24 @@ __device__ __forceinline__ void fp_block(const FpArgs& L, int t) {
     // layered texture is given, so both units share the work
     const bool use_tex = L.vtex && L.rank[A] == 2 && !(__ldg(&P->flags) & KK_FP_NO_TEXTURE);
     if (use_tex && a_fast)
-        fp_trace<TV, TP, TEX8, EPI, 3, 0, true>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
+        fp_trace<TV, TP, TEX8, EPI, 3, 0, true, SUMS>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
     else if (use_tex)
-        fp_trace<TV, TP, TEX8, EPI, 3, 0, false>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
+        fp_trace<TV, TP, TEX8, EPI, 3, 0, false, SUMS>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
     else if (shared && rule == 1)
-        fp_trace<TV, TP, TEX8, EPI, 2, 1>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
+        fp_trace<TV, TP, TEX8, EPI, 2, 1, false, SUMS>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
     else if (shared)
-        fp_trace<TV, TP, TEX8, EPI, 2, 0>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
+        fp_trace<TV, TP, TEX8, EPI, 2, 0, false, SUMS>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
     else if (fast && rule == 1)
-        fp_trace<TV, TP, TEX8, EPI, 1, 1>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
+        fp_trace<TV, TP, TEX8, EPI, 1, 1, false, SUMS>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
     else if (fast)
-        fp_trace<TV, TP, TEX8, EPI, 1, 0>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
+        fp_trace<TV, TP, TEX8, EPI, 1, 0, false, SUMS>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
     else
-        fp_trace<TV, TP, TEX8, EPI, 0, 0>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
+        fp_trace<TV, TP, TEX8, EPI, 0, 0, false, SUMS>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
 }
 
-template <typename TV, typename TP, bool TEX8, int EPI>
+template <typename TV, typename TP, bool TEX8, int EPI, bool SUMS = false>
 __global__ void __launch_bounds__(32 * FP_COLS, KK_FP_MINBLOCKS) cone_fp_kernel(const FpArgs L) {
-    fp_block<TV, TP, TEX8, EPI>(L, blockIdx.x);
+    fp_block<TV, TP, TEX8, EPI, SUMS>(L, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -846,9 +846,9 @@ static bool launch_fp_sums(const FpArgs& base, bool tex8, cudaStream_t s, const 
             L.store_sums = p < passes - 1;
             L.final_pass = p == passes - 1;
             if (tex8)
-                cone_fp_kernel<TV, TP, true, EPI><<<(unsigned)blocks, 32 * FP_COLS, 0, s>>>(L);
+                cone_fp_kernel<TV, TP, true, EPI, true><<<(unsigned)blocks, 32 * FP_COLS, 0, s>>>(L);
             else
-                cone_fp_kernel<TV, TP, false, EPI><<<(unsigned)blocks, 32 * FP_COLS, 0, s>>>(L);
+                cone_fp_kernel<TV, TP, false, EPI, true><<<(unsigned)blocks, 32 * FP_COLS, 0, s>>>(L);
         }
     }
     return true;

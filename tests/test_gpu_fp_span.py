@@ -130,7 +130,12 @@ def test_residual_partial_overlap_is_rejected():
 def test_16bit_projection_spans_through_the_sums_buffer(vdt, half_tex, mode):
     """float16 projections traced in 16-slice spans whose float32 running
     sums pass through the caller's buffer (whole scan, or chunks of 5 and
-    of 1 angles) equal the one-launch result bit for bit."""
+    of 1 angles) equal the one-launch result bit for bit. (The residual
+    epilogue takes 16-bit volumes with float16 projections, or float32
+    with float32.)"""
+    if vdt == torch.float32 and mode.startswith("residual"):
+        pytest.skip("residual epilogue: float32 volume with float16 "
+                    "projections is not a supported storage pair")
     pgs, vg = build_case("config1")
     vol = torch.from_numpy(case_volume("config1", vg)).cuda().to(vdt)
     det = pgs[0].detector
