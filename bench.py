@@ -491,10 +491,14 @@ def run_batched(n_problems=32, iters=30, seed=1237):
             "rel_l2_phantom": {"min": min(rels),
                                "median": float(np.median(rels)),
                                "max": max(rels)},
-            "launches_per_iter": "1 FP + 1 BP per 32-angle chunk index "
-                                 "(+ texture refills); all iterations in "
-                                 "one CUDA graph",
-            "autotuned": {"fp_axis_group": sorted(set(tuner.cache.values()))}}
+            "launches_per_iter": "1 FP launch per slice span + 1 persistent "
+                                 "BP launch (+ texture refills); all "
+                                 "iterations in one CUDA graph",
+            "autotuned": {kind: sorted({json.dumps(v) for k, v in
+                                        tuner.cache.items()
+                                        if k.startswith(kind + ":")})
+                          for kind in ("fp_axis_group", "fp_span",
+                                       "bp_tile")}}
 
 
 def run_sirt_config5(iters=20, seed=1239):
