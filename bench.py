@@ -998,6 +998,64 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_profile_op(args):
+    """One operator, twice (the second is the one a profiler captures),
+    on the chosen workload: ``fp`` (``--fp-tiles`` / ``--fp-no-texture``
+    select its paths), ``bp``, ``fdk`` (pre-processing fused with the
+    texture store, then the chunked BP) or ``adjoint`` (the exact
+    transpose of the FP). Prints the second run's CUDA-event time."""
+    import torch
+
+    from kernelkit import _native, algo
+    from kernelkit.kernels import RayDrivenConeFP, VoxelDrivenConeBP
+
+    w = WORKLOADS[args.workload]
+    pgs, vg = make_scan(w)
+    vol = make_volume(w, vg)
+    det = w["det"]
+    proj = torch.empty((len(pgs), det, det), device="cuda")
+    fp = RayDrivenConeFP(use_texture_unit=not args.fp_no_texture)
+    fp.use_tiles = bool(args.fp_tiles)
+    fp.compile()
+    fp.set_params(fp.geoms2params(pgs, vg))
+    fp(vol, pgs, vg, proj, additive=False)
+    if args.profile_op == "fp":
+        def op():
+            fp(vol, pgs, vg, proj, additive=False)
+    elif args.profile_op == "bp":
+        bp = VoxelDrivenConeBP()
+        bp.compile()
+        bp.set_params(bp.geoms2params(pgs, vg))
+        tex = _native.Layered(len(pgs), det, det, _native.KK_F32)
+        tex.copy_from(proj)
+        out = torch.empty_like(vol)
+
+        def op():
+            bp(tex, out, vg, additive=False)
+    elif args.profile_op == "fdk":
+        work = torch.empty_like(proj)
+
+        def op():
+            work.copy_(proj)
+            algo._streamed_bp(work, pgs, vg, "ramlak")
+    else:
+        out = torch.empty_like(vol)
+
+        def op():
+            fp.transpose(proj, pgs, vg, out)
+    op()
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    op()
+    b.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_op": args.profile_op, "workload": args.workload,
+                      "ms": a.elapsed_time(b),
+                      "wait_timeouts": _native.wait_timeouts()}), flush=True)
+
+
 def run_reference(args):
     """Reference arm: the oracle's restatement of the reference algorithm
     (the reference itself has no CPU path; its GPU kernels are exercised by
@@ -1062,7 +1120,18 @@ def main(argv=None):
     ap.add_argument("--no-sirt", action="store_true",
                     help="skip the SIRT measurements (config 2 and the "
                          "batched config 4)")
+    ap.add_argument("--profile-op", choices=("fp", "bp", "fdk", "adjoint"),
+                    help="only run one operator twice on the workload (for "
+                         "profiler captures; prints its own JSON line)")
+    ap.add_argument("--fp-tiles", action="store_true",
+                    help="--profile-op fp: shared-memory tiles for the "
+                         "CUDA-core rays")
+    ap.add_argument("--fp-no-texture", action="store_true",
+                    help="--profile-op fp: every ray on the CUDA cores")
     args = ap.parse_args(argv)
+    if args.profile_op:
+        run_profile_op(args)
+        return
     if args.sirt_config5:
         print(json.dumps(run_sirt_config5()), flush=True)
         return
