@@ -319,10 +319,16 @@ static void launch_bp_typed(const BpArgs& L, bool tex8, cudaStream_t s) {
 // when it is float32 and the result is a plain sum; otherwise in the
 // float32 work buffer (when given). Without a buffer in those cases a
 // single launch covers every angle (same arithmetic, more L2 traffic).
+// 32-angle chunks per launch (each chunk's sum still added on its own)
+#ifndef KK_BP_CHUNKS_PER_LAUNCH
+#define KK_BP_CHUNKS_PER_LAUNCH 1
+#endif
+constexpr int BP_LAUNCH_ANGLES = BP_CHUNK * KK_BP_CHUNKS_PER_LAUNCH;
+
 template <typename Fn>
 static void bp_chunks(BpArgs L, bool vol_f32, bool additive, bool update, Fn one) {
     const int n = L.n_angles;
-    const int chunks = (n + BP_CHUNK - 1) / BP_CHUNK;
+    const int chunks = (n + BP_LAUNCH_ANGLES - 1) / BP_LAUNCH_ANGLES;
     const bool need_work = chunks > 1 && (!vol_f32 || update);
     const int first_load = (additive && !update) ? LOAD_VOL : LOAD_ZERO;
     if (need_work && !L.work) {
@@ -334,8 +340,8 @@ static void bp_chunks(BpArgs L, bool vol_f32, bool additive, bool update, Fn one
         return;
     }
     for (int c = 0; c < chunks; ++c) {
-        L.j_begin = c * BP_CHUNK;
-        L.j_end = min(n, L.j_begin + BP_CHUNK);
+        L.j_begin = c * BP_LAUNCH_ANGLES;
+        L.j_end = min(n, L.j_begin + BP_LAUNCH_ANGLES);
         L.load_mode = c == 0 ? first_load : (need_work ? LOAD_WORK : LOAD_VOL);
         L.store_mode = c == chunks - 1 ? STORE_FINAL : (need_work ? STORE_WORK : STORE_VOL);
         one(L);

@@ -173,24 +173,36 @@ __global__ void __launch_bounds__(FFT_THREADS)
     const int line0 = 2 * blockIdx.x;
     const bool two = line0 + 1 < n_lines;
     const int a0 = line0 / rows, r0 = line0 % rows;
-    const int a1 = (line0 + 1) / rows, r1 = (line0 + 1) % rows;
+    // a block with a single row (odd row count) repeats it as the second
+    // one, which is never stored
+    const int a1 = two ? (line0 + 1) / rows : a0, r1 = two ? (line0 + 1) % rows : r0;
     const float* row0 = (src_table ? (const float*)src_table[a0] : src + (int64_t)a0 * sa) + (int64_t)r0 * sr;
     const float* row1 = (src_table ? (const float*)src_table[a1] : src + (int64_t)a1 * sa) + (int64_t)r1 * sr;
     const double* g0 = geom ? geom + 13 * (int64_t)a0 : nullptr;
     const double* g1 = geom ? geom + 13 * (int64_t)a1 : nullptr;
-    for (int j = tid; j < P; j += FFT_THREADS) {
-        double re = 0.0, im = 0.0;
-        if (j < cols) {
-            re = fdk_load(row0, sc, j, r0, g0);
-            if (two) im = fdk_load(row1, sc, j, r1, g1);
-        }
-        fz[fpad(j)] = make_double2(re, im);
-    }
-    __syncthreads();
-    // forward: radix-4 decimation in frequency, then radix 2 if log2 P is odd
+    auto load = [&](int j) -> double2 {
+        if (j >= cols) return make_double2(0.0, 0.0);
+        return make_double2(fdk_load(row0, sc, j, r0, g0), two ? fdk_load(row1, sc, j, r1, g1) : 0.0);
+    };
     const double2* tw = reinterpret_cast<const double2*>(plan + P);  // stage records
-    int len = P, lq = log2P - 2;  // lq = log2(len / 4)
-    for (; len >= 4; tw += (len >> 2), len >>= 2, lq -= 2) {
+    const int q0 = P >> 2;
+    // forward stage of length P fused with the load: inputs j + 2 P/4 and
+    // j + 3 P/4 are zero padding (P >= 2 cols)
+    for (int j = tid; j < q0; j += FFT_THREADS) {
+        const double2 a = load(j), b = load(j + q0);
+        const double2 w1 = __ldg(&tw[j]), w2 = cmul(w1, w1), w3 = cmul(w2, w1);
+        const double2 t3 = make_double2(b.y, -b.x);  // b * (-i)
+        fz[fpad(j)] = cadd(a, b);
+        fz[fpad(j + q0)] = cmul(csub(a, b), w2);
+        fz[fpad(j + 2 * q0)] = cmul(cadd(a, t3), w1);
+        fz[fpad(j + 3 * q0)] = cmul(csub(a, t3), w3);
+    }
+    tw += q0;
+    __syncthreads();
+    // the middle forward stages: radix-4 decimation in frequency
+    const int lastlen = (log2P & 1) ? 2 : 4;
+    int len = P >> 2, lq = log2P - 4;  // lq = log2(len / 4)
+    for (; len > lastlen; tw += (len >> 2), len >>= 2, lq -= 2) {
         const int q = len >> 2;
         for (int t = tid; t < (P >> 2); t += FFT_THREADS) {
             const int j = t & (q - 1), base = ((t >> lq) * len) + j;
@@ -207,35 +219,47 @@ __global__ void __launch_bounds__(FFT_THREADS)
         }
         __syncthreads();
     }
-    if (len == 2) {
+    // the last forward stage, the product with H (plan order: bit-reversed,
+    // as the spectrum) and the first inverse stage, on the same groups of
+    // consecutive elements (its twiddles are 1)
+    if (lastlen == 2) {
         for (int t = tid; t < (P >> 1); t += FFT_THREADS) {
             const double2 u = fz[fpad(2 * t)], v = fz[fpad(2 * t + 1)];
-            fz[fpad(2 * t)] = cadd(u, v);
-            fz[fpad(2 * t + 1)] = csub(u, v);
+            const double h0 = __ldg(&plan[2 * t]), h1 = __ldg(&plan[2 * t + 1]);
+            const double2 p0 = cadd(u, v), p1 = csub(u, v);
+            const double2 f0 = make_double2(p0.x * h0, p0.y * h0), f1 = make_double2(p1.x * h1, p1.y * h1);
+            fz[fpad(2 * t)] = cadd(f0, f1);
+            fz[fpad(2 * t + 1)] = csub(f0, f1);
         }
-        __syncthreads();
-    }
-    // filter: the spectrum and the plan's H are in bit-reversed order
-    for (int i = tid; i < P; i += FFT_THREADS) {
-        const double h = __ldg(&plan[i]);
-        const double2 v = fz[fpad(i)];
-        fz[fpad(i)] = make_double2(v.x * h, v.y * h);
+    } else {
+        for (int t = tid; t < (P >> 2); t += FFT_THREADS) {
+            const int base = 4 * t;
+            const double2 a = fz[fpad(base)], b = fz[fpad(base + 1)], c = fz[fpad(base + 2)], d = fz[fpad(base + 3)];
+            const double2 t0 = cadd(a, c), t1 = csub(a, c), t2 = cadd(b, d);
+            const double2 bd = csub(b, d);
+            const double2 t3 = make_double2(bd.y, -bd.x);
+            double2 y[4] = {cadd(t0, t2), csub(t0, t2), cadd(t1, t3), csub(t1, t3)};
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                const double h = __ldg(&plan[base + m]);
+                y[m] = make_double2(y[m].x * h, y[m].y * h);
+            }
+            // inverse of the stage: y0, y2, y1, y3 sit at base, +1, +2, +3
+            const double2 s0 = cadd(y[0], y[1]), s2 = csub(y[0], y[1]), s1 = cadd(y[2], y[3]);
+            const double2 dd = csub(y[2], y[3]);
+            const double2 s3 = make_double2(-dd.y, dd.x);  // (y1 - y3) * i
+            fz[fpad(base)] = cadd(s0, s1);
+            fz[fpad(base + 1)] = cadd(s2, s3);
+            fz[fpad(base + 2)] = csub(s0, s1);
+            fz[fpad(base + 3)] = csub(s2, s3);
+        }
+        tw += 1;  // the length-4 stage's record (its twiddle is 1)
     }
     __syncthreads();
-    // inverse: the stages above undone in reverse order, conjugate
-    // twiddles, unnormalised (the result is P times the filtered signal)
-    len = 4;
-    if (log2P & 1) {
-        for (int t = tid; t < (P >> 1); t += FFT_THREADS) {
-            const double2 u = fz[fpad(2 * t)], v = fz[fpad(2 * t + 1)];
-            fz[fpad(2 * t)] = cadd(u, v);
-            fz[fpad(2 * t + 1)] = csub(u, v);
-        }
-        __syncthreads();
-        len = 8;
-    }
-    // the stage records in reverse: tw points just past the last one
-    for (lq = (len == 4 ? 0 : 1); len <= P; len <<= 2, lq += 2) {
+    // the middle inverse stages: conjugate twiddles, reverse order,
+    // unnormalised (the result is P times the filtered signal)
+    if (lastlen == 4) tw -= 1;
+    for (len = lastlen * 4, lq = (lastlen == 4 ? 2 : 1); len <= (P >> 2); len <<= 2, lq += 2) {
         const int q = len >> 2;
         tw -= q;
         for (int t = tid; t < (P >> 2); t += FFT_THREADS) {
@@ -255,12 +279,14 @@ __global__ void __launch_bounds__(FFT_THREADS)
         }
         __syncthreads();
     }
-    // the first cols values, scaled by 1 / P (exact: P is a power of two)
+    // the inverse stage of length P fused with the store of the first cols
+    // values (outputs j and j + P/4; the other two lie beyond P/2 >= cols),
+    // scaled by 1 / P (exact: P is a power of two)
+    tw -= q0;
     const double inv = 1.0 / (double)P;
     float* out0 = dst ? (dst_table ? (float*)dst_table[a0] : dst + (int64_t)a0 * da) + (int64_t)r0 * dr : nullptr;
     float* out1 = dst ? (dst_table ? (float*)dst_table[a1] : dst + (int64_t)a1 * da) + (int64_t)r1 * dr : nullptr;
-    for (int j = tid; j < cols; j += FFT_THREADS) {
-        const double2 v = fz[fpad(j)];
+    auto store = [&](int j, double2 v) {
         const float f0 = __double2float_rn(v.x * inv);
         if (out0) out0[(int64_t)j * dc] = f0;
         if (surf) surf2DLayeredwrite(f0, surf, j * (int)sizeof(float), r0, layer0 + a0);
@@ -269,6 +295,18 @@ __global__ void __launch_bounds__(FFT_THREADS)
             if (out1) out1[(int64_t)j * dc] = f1;
             if (surf) surf2DLayeredwrite(f1, surf, j * (int)sizeof(float), r1, layer0 + a1);
         }
+    };
+    for (int j = tid; j < q0 && j < cols; j += FFT_THREADS) {
+        const double2 w1 = __ldg(&tw[j]), w2 = cmul(w1, w1), w3 = cmul(w2, w1);
+        const double2 y0 = fz[fpad(j)];
+        const double2 y2 = cmulc(fz[fpad(j + q0)], w2);
+        const double2 y1 = cmulc(fz[fpad(j + 2 * q0)], w1);
+        const double2 y3 = cmulc(fz[fpad(j + 3 * q0)], w3);
+        const double2 t0 = cadd(y0, y2), t2 = csub(y0, y2), t1 = cadd(y1, y3);
+        const double2 dd = csub(y1, y3);
+        const double2 t3 = make_double2(-dd.y, dd.x);
+        store(j, cadd(t0, t1));
+        if (j + q0 < cols) store(j + q0, cadd(t2, t3));
     }
 }
 
