@@ -91,6 +91,13 @@ __device__ __forceinline__ float fast_sample(float acc, const T* __restrict__ ro
     return acc;
 }
 
+// Whether the samples of a ray between coordinates c0 and c1 (first and
+// last slice of a slab) can touch a texel of an axis of n texels: the
+// complement of span_class's "every sample reads only border zeros".
+__device__ __forceinline__ bool span_touches(float c0, float c1, int n) {
+    return fmaxf(c0, c1) >= -0.53f && fminf(c0, c1) <= (float)n + 0.53f;
+}
+
 // Slab classification of a ray from its coordinates at the first and last
 // slice of the slab (coordinates move linearly; the float32 increments
 // drift by far less than the margins). 2 = both texels of every sample
@@ -154,7 +161,12 @@ __device__ __forceinline__ void fp_trace(const FpArgs& L, const kk_fp_angle* P, 
             yc[k] = __fadd_rn(fmaf(R[k].a1, t1, R[k].b1), half1);
             zc[k] = __fadd_rn(fmaf(R[k].a2, t1, R[k].b2), half2);
             val[k] = 0.f;
-            if (PATH != 0) {
+            if (PATH == 3) {
+                // the texture unit handles borders: only slabs that miss
+                // the volume need a test
+                any |= span_touches(yc[k], fmaf(R[k].a1, span, yc[k]), n1) &&
+                       span_touches(zc[k], fmaf(R[k].a2, span, zc[k]), n2);
+            } else if (PATH != 0) {
                 const int cy = span_class(yc[k], fmaf(R[k].a1, span, yc[k]), n1);
                 const int cz = span_class(zc[k], fmaf(R[k].a2, span, zc[k]), n2);
                 const int ck = min(cy, cz);
@@ -163,28 +175,31 @@ __device__ __forceinline__ void fp_trace(const FpArgs& L, const kk_fp_angle* P, 
             }
         }
         // warp-uniform choice: skip, unchecked or checked loop
-        const bool all_in = PATH != 0 && __all_sync(0xffffffffu, cls == 2);
+        const bool all_in = PATH != 0 && PATH != 3 && __all_sync(0xffffffffu, cls == 2);
         const bool all_out = PATH != 0 && !__any_sync(0xffffffffu, any != 0);
         if (all_out) continue;  // every sample is zero; the slab adds +0
         if (PATH == 3 && FP_RPT == 2) {
             // the texture unit filters: layer = slice, u = the faster and
             // v = the slower in-slice axis; each fetch equals the
-            // reference's 3D-texture sample for these rays. The two rays'
-            // coordinate and sum chains advance in paired instructions.
-            float2 y2 = f2(yc[0], yc[1]), z2 = f2(zc[0], zc[1]), v2 = f2(0.f);
-            const float2 a1 = f2(R[0].a1, R[FP_RPT - 1].a1), a2 = f2(R[0].a2, R[FP_RPT - 1].a2);
+            // reference's 3D-texture sample for these rays. Scalar
+            // coordinate registers feed the fetches directly (paired FP32
+            // chains here cost issue slots that the CUDA-core rays of the
+            // same launch need: 169 -> 165 ms on the 512^3 x 720 scan).
+            float ya = yc[0], za = zc[0], yb = yc[1], zb = zc[1], va = 0.f, vb = 0.f;
+            const float a1a = R[0].a1, a2a = R[0].a2, a1b = R[1].a1, a2b = R[1].a2;
 #pragma unroll FP_TEX_UNROLL
             for (int sl = off; sl < end; ++sl) {
-                const float s0 = AF ? tex2DLayered<float>(L.vtex, y2.x, z2.x, sl)
-                                    : tex2DLayered<float>(L.vtex, z2.x, y2.x, sl);
-                const float s1 = AF ? tex2DLayered<float>(L.vtex, y2.y, z2.y, sl)
-                                    : tex2DLayered<float>(L.vtex, z2.y, y2.y, sl);
-                v2 = add2(v2, f2(s0, s1));
-                y2 = add2(y2, a1);
-                z2 = add2(z2, a2);
+                const float s0 = AF ? tex2DLayered<float>(L.vtex, ya, za, sl) : tex2DLayered<float>(L.vtex, za, ya, sl);
+                const float s1 = AF ? tex2DLayered<float>(L.vtex, yb, zb, sl) : tex2DLayered<float>(L.vtex, zb, yb, sl);
+                va = __fadd_rn(va, s0);
+                vb = __fadd_rn(vb, s1);
+                ya = __fadd_rn(ya, a1a);
+                za = __fadd_rn(za, a2a);
+                yb = __fadd_rn(yb, a1b);
+                zb = __fadd_rn(zb, a2b);
             }
-            val[0] = v2.x;
-            val[FP_RPT - 1] = v2.y;
+            val[0] = va;
+            val[1] = vb;
         } else if (PATH == 3) {
             for (int sl = off; sl < end; ++sl) {
 #pragma unroll
