@@ -62,6 +62,9 @@ struct FpArgs {
     float* sums;
     int load_sums;   // start from sums (later launches)
     int store_sums;  // leave the sums there (all but the last launch)
+    // vol is the interior of a copy with two zero texels before and after
+    // every axis (the border rule as memory)
+    int padded;
 };
 
 struct BpArgs {

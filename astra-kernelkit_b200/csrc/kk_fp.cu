@@ -31,6 +31,12 @@ namespace kk {
 #ifndef KK_FP_MINBLOCKS
 #define KK_FP_MINBLOCKS 6
 #endif
+#ifndef KK_FP_PAD_MINBLOCKS
+#define KK_FP_PAD_MINBLOCKS 5  // the padded-copy kernel: 48 registers, no spills
+#endif
+#ifndef KK_FP_PAD_TEX_UNROLL
+#define KK_FP_PAD_TEX_UNROLL 8  // its texture loop (4 in the 40-register kernel)
+#endif
 #ifndef KK_FP_TEX_UNROLL
 #define KK_FP_TEX_UNROLL 4  // slices per unrolled step of the texture loop
 #endif
@@ -40,6 +46,7 @@ namespace kk {
 constexpr int FP_RPT = KK_FP_RPT;       // rays per thread
 constexpr int FP_UNROLL = KK_FP_UNROLL;
 constexpr int FP_TEX_UNROLL = KK_FP_TEX_UNROLL;
+constexpr int FP_PAD_TEX_UNROLL = KK_FP_PAD_TEX_UNROLL;
 constexpr int FP_COLS = 8;              // columns per block (one per warp)
 constexpr int FP_ROWS_T = 32 * FP_RPT;  // rows per block
 
@@ -112,7 +119,8 @@ __device__ __forceinline__ int span_class(float c0, float c1, int n) {
     return 1;
 }
 
-template <typename TV, typename TP, bool TEX8, int EPI, int PATH, int RULE, bool AF = false, bool SUMS = false>
+template <typename TV, typename TP, bool TEX8, int EPI, int PATH, int RULE, bool AF = false, bool SUMS = false,
+          bool PAD = false>
 __device__ __forceinline__ void fp_trace(const FpArgs& L, const kk_fp_angle* P, int rec, int a, int A, int D1, int D2,
                                          int rule, bool a_fast, int r0, int c, int lane) {
     float src[3], cor[3], u[3], v[3];
@@ -187,7 +195,7 @@ __device__ __forceinline__ void fp_trace(const FpArgs& L, const kk_fp_angle* P, 
             // same launch need: 169 -> 165 ms on the 512^3 x 720 scan).
             float ya = yc[0], za = zc[0], yb = yc[1], zb = zc[1], va = 0.f, vb = 0.f;
             const float a1a = R[0].a1, a2a = R[0].a2, a1b = R[1].a1, a2b = R[1].a2;
-#pragma unroll FP_TEX_UNROLL
+#pragma unroll(PAD ? FP_PAD_TEX_UNROLL : FP_TEX_UNROLL)
             for (int sl = off; sl < end; ++sl) {
                 const float s0 = AF ? tex2DLayered<float>(L.vtex, ya, za, sl) : tex2DLayered<float>(L.vtex, za, ya, sl);
                 const float s1 = AF ? tex2DLayered<float>(L.vtex, yb, zb, sl) : tex2DLayered<float>(L.vtex, zb, yb, sl);
@@ -222,51 +230,69 @@ __device__ __forceinline__ void fp_trace(const FpArgs& L, const kk_fp_angle* P, 
                     zc[k] = __fadd_rn(zc[k], R[k].a2);
                 }
             }
-        } else if (TEX8 && PATH == 2 && FP_RPT == 2 && all_in && L.off32) {
+        } else if (TEX8 && PATH == 2 && FP_RPT == 2 && (PAD || (all_in && L.off32))) {
             // Both rays of the thread share the D1 coordinate (and so its
             // split and the two D1 rows); their D2 samples run in paired
             // instructions. Element offsets fit 32 bits (checked on the
             // host); the split's 0x4B4000 bias is folded into the row
             // offset. Same operations, order and rounding as fast_sample.
-            float2 z2 = f2(zc[0], zc[1]), v2 = f2(0.f);
-            const float2 a2 = f2(R[0].a2, R[FP_RPT - 1].a2);
-            float y = yc[0];
-            const float a1 = R[0].a1;
-            const TV* vol1 = vol + st1;
-            const int st1i = (int)st1, sSi = (int)sS;
-            int soff = off * sSi - 0x4B4000;
+            // CLAMP (mixed slabs of a volume with two zero texels around
+            // it): the coordinates that feed the split are clamped to
+            // [-1.5, n + 1.5 - 1/256], which changes no coordinate whose
+            // texels can be non-zero and keeps every texel index in
+            // [-2, n + 1], so the loads need no test: texels outside the
+            // volume read the padding's zeros, as the border does.
+            auto shared_loop = [&](auto clamp_tag) {
+                constexpr bool CLAMP = decltype(clamp_tag)::value;
+                float2 z2 = f2(zc[0], zc[1]), v2 = f2(0.f);
+                const float2 a2 = f2(R[0].a2, R[FP_RPT - 1].a2);
+                float y = yc[0];
+                const float a1 = R[0].a1;
+                const float yhi = (float)n1 + 1.49609375f, zhi = (float)n2 + 1.49609375f;
+                const TV* vol1 = vol + st1;
+                const int st1i = (int)st1, sSi = (int)sS;
+                int soff = off * sSi - 0x4B4000;
 #pragma unroll FP_UNROLL
-            for (int sl = off; sl < end; ++sl, soff += sSi) {
-                const int yb = __float_as_int(__fadd_rd(__fmaf_rd(y, 256.f, -127.5f), 12582912.f));
-                const int rowoff = ((yb >> 8) - 0x4B4000) * st1i + soff;
-                const float S = __int_as_float((yb & 255) | 0x4B000000) - 8388608.f;
-                const float S256 = S * (1.f / 256.f);
-                const float2 m = add2_rd(fma2_rd(z2, f2(256.f), f2(-127.5f)), f2(12582912.f));
-                const int b0 = __float_as_int(m.x), b1 = __float_as_int(m.y);
-                const int o0 = (b0 >> 8) + rowoff, o1 = (b1 >> 8) + rowoff;
-                const float2 t00 = f2(ld(vol + o0), ld(vol + o1));
-                const float2 t10 = f2(ld(vol + o0 + 1), ld(vol + o1 + 1));
-                const float2 t01 = f2(ld(vol1 + o0), ld(vol1 + o1));
-                const float2 t11 = f2(ld(vol1 + o0 + 1), ld(vol1 + o1 + 1));
-                // Fr = 2^23 + F, F the fast weight (0..255)
-                const float2 Fr = f2(__int_as_float((b0 & 255) | 0x4B000000), __int_as_float((b1 & 255) | 0x4B000000));
-                const float2 F = add2(Fr, f2(-8388608.f));
-                // x1 = floor(F S / 256 + 1/2), all steps exact
-                const float2 x1 = add2(add2_rd(fma2(F, f2(S256), f2(0.5f)), f2(12582912.f)), f2(-12582912.f));
-                float2 x0;
-                if (RULE == 1)  // F + floor(1/2 - F S / 256); Fr - 2.5 * 2^23 = F - 1.5 * 2^23
-                    x0 = add2(add2_rd(fma2(F, f2(-S256), f2(0.5f)), f2(12582912.f)), add2(Fr, f2(-20971520.f)));
-                else
-                    x0 = sub2(F, x1);
-                v2 = fma2(f2(256.f), t00, v2);
-                v2 = fma2(f2(S), sub2(t01, t00), v2);
-                v2 = fma2(x1, sub2(t11, t01), v2);
-                v2 = fma2(x0, sub2(t10, t00), v2);
-                z2 = add2(z2, a2);
-                y = __fadd_rn(y, a1);
-            }
-            val[0] = v2.x;
-            val[FP_RPT - 1] = v2.y;
+                for (int sl = off; sl < end; ++sl, soff += sSi) {
+                    const float ys = CLAMP ? fminf(fmaxf(y, -1.5f), yhi) : y;
+                    const int yb = __float_as_int(__fadd_rd(__fmaf_rd(ys, 256.f, -127.5f), 12582912.f));
+                    const int rowoff = ((yb >> 8) - 0x4B4000) * st1i + soff;
+                    const float S = __int_as_float((yb & 255) | 0x4B000000) - 8388608.f;
+                    const float S256 = S * (1.f / 256.f);
+                    const float2 zs =
+                        CLAMP ? f2(fminf(fmaxf(z2.x, -1.5f), zhi), fminf(fmaxf(z2.y, -1.5f), zhi)) : z2;
+                    const float2 m = add2_rd(fma2_rd(zs, f2(256.f), f2(-127.5f)), f2(12582912.f));
+                    const int b0 = __float_as_int(m.x), b1 = __float_as_int(m.y);
+                    const int o0 = (b0 >> 8) + rowoff, o1 = (b1 >> 8) + rowoff;
+                    const float2 t00 = f2(ld(vol + o0), ld(vol + o1));
+                    const float2 t10 = f2(ld(vol + o0 + 1), ld(vol + o1 + 1));
+                    const float2 t01 = f2(ld(vol1 + o0), ld(vol1 + o1));
+                    const float2 t11 = f2(ld(vol1 + o0 + 1), ld(vol1 + o1 + 1));
+                    // Fr = 2^23 + F, F the fast weight (0..255)
+                    const float2 Fr =
+                        f2(__int_as_float((b0 & 255) | 0x4B000000), __int_as_float((b1 & 255) | 0x4B000000));
+                    const float2 F = add2(Fr, f2(-8388608.f));
+                    // x1 = floor(F S / 256 + 1/2), all steps exact
+                    const float2 x1 = add2(add2_rd(fma2(F, f2(S256), f2(0.5f)), f2(12582912.f)), f2(-12582912.f));
+                    float2 x0;
+                    if (RULE == 1)  // F + floor(1/2 - F S / 256); Fr - 2.5 * 2^23 = F - 1.5 * 2^23
+                        x0 = add2(add2_rd(fma2(F, f2(-S256), f2(0.5f)), f2(12582912.f)), add2(Fr, f2(-20971520.f)));
+                    else
+                        x0 = sub2(F, x1);
+                    v2 = fma2(f2(256.f), t00, v2);
+                    v2 = fma2(f2(S), sub2(t01, t00), v2);
+                    v2 = fma2(x1, sub2(t11, t01), v2);
+                    v2 = fma2(x0, sub2(t10, t00), v2);
+                    z2 = add2(z2, a2);
+                    y = __fadd_rn(y, a1);
+                }
+                val[0] = v2.x;
+                val[FP_RPT - 1] = v2.y;
+            };
+            if (all_in)
+                shared_loop(std::false_type{});
+            else if constexpr (PAD)
+                shared_loop(std::true_type{});
         } else if (all_in) {
 #pragma unroll FP_UNROLL
             for (int sl = off; sl < end; ++sl) {
@@ -333,7 +359,11 @@ __device__ __forceinline__ void fp_trace(const FpArgs& L, const kk_fp_angle* P, 
     }
 }
 
-template <typename TV, typename TP, bool TEX8, int EPI, bool SUMS = false>
+// PAD: the instance for a zero-padded volume copy (FpArgs.padded, offsets
+// in 32 bits), whose shared-D1 rays trace mixed slabs with the clamped
+// paired loop; a separate kernel with its own register budget keeps the
+// other kernels' allocation as it was.
+template <typename TV, typename TP, bool TEX8, int EPI, bool SUMS = false, bool PAD = false>
 __device__ __forceinline__ void fp_block(const FpArgs& L, int t) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int ct = t % L.col_tiles;
@@ -359,13 +389,13 @@ __device__ __forceinline__ void fp_block(const FpArgs& L, int t) {
     // layered texture is given, so both units share the work
     const bool use_tex = L.vtex && L.rank[A] == 2 && !(__ldg(&P->flags) & KK_FP_NO_TEXTURE);
     if (use_tex && a_fast)
-        fp_trace<TV, TP, TEX8, EPI, 3, 0, true, SUMS>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
+        fp_trace<TV, TP, TEX8, EPI, 3, 0, true, SUMS, PAD>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
     else if (use_tex)
-        fp_trace<TV, TP, TEX8, EPI, 3, 0, false, SUMS>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
+        fp_trace<TV, TP, TEX8, EPI, 3, 0, false, SUMS, PAD>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
     else if (shared && rule == 1)
-        fp_trace<TV, TP, TEX8, EPI, 2, 1, false, SUMS>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
+        fp_trace<TV, TP, TEX8, EPI, 2, 1, false, SUMS, PAD>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
     else if (shared)
-        fp_trace<TV, TP, TEX8, EPI, 2, 0, false, SUMS>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
+        fp_trace<TV, TP, TEX8, EPI, 2, 0, false, SUMS, PAD>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
     else if (fast && rule == 1)
         fp_trace<TV, TP, TEX8, EPI, 1, 1, false, SUMS>(L, P, rec, a, A, D1, D2, rule, a_fast, r0, c, lane);
     else if (fast)
@@ -377,6 +407,12 @@ __device__ __forceinline__ void fp_block(const FpArgs& L, int t) {
 template <typename TV, typename TP, bool TEX8, int EPI, bool SUMS = false>
 __global__ void __launch_bounds__(32 * FP_COLS, KK_FP_MINBLOCKS) cone_fp_kernel(const FpArgs L) {
     fp_block<TV, TP, TEX8, EPI, SUMS>(L, blockIdx.x);
+}
+
+// cone_fp_kernel on a zero-padded volume copy (texture-compatible weights)
+template <typename TV, typename TP, int EPI>
+__global__ void __launch_bounds__(32 * FP_COLS, KK_FP_PAD_MINBLOCKS) cone_fp_pad_kernel(const FpArgs L) {
+    fp_block<TV, TP, true, EPI, false, true>(L, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -898,6 +934,8 @@ static void launch_fp_typed(const FpArgs& base, bool tex8, cudaStream_t s, const
         if (brick) {
             Bl.L = L;
             cone_fp_brick_kernel<EPI><<<(unsigned)blocks, 32 * BRICK_WARPS, BRICK_SMEM, s>>>(Bl);
+        } else if (tex8 && L.padded) {
+            cone_fp_pad_kernel<TV, TP, EPI><<<(unsigned)blocks, 32 * FP_COLS, 0, s>>>(L);
         } else if (tex8) {
             cone_fp_kernel<TV, TP, true, EPI><<<(unsigned)blocks, 32 * FP_COLS, 0, s>>>(L);
         } else {
@@ -926,6 +964,58 @@ static int launch_fp(const FpArgs& L, int vdt, int pdt, bool tex8, cudaStream_t 
     }
 #undef KK_FP_CASE
     return kk_fail(KK_ERR_UNSUPPORTED, "kk_cone_fp: dtype combination volume=%d projections=%d", vdt, pdt);
+}
+
+// The zero-padded copy: dst holds the volume with two zero texels before
+// and after every axis, in C order over the memory ranks (extents n[r] + 4,
+// rank 0 fastest); src has the volume's own strides (per rank). Block (x,
+// padded row along rank 1, padded plane along rank 2), threads along the
+// padded rank-0 row, so both sides stream.
+template <typename T>
+__global__ void fp_pad_kernel(const T* __restrict__ src, T* __restrict__ dst, int n0, int n1, int n2, int64_t s0,
+                              int64_t s1, int64_t s2) {
+    const int m0 = n0 + 4;
+    const int i1 = (int)blockIdx.y - 2, i2 = (int)blockIdx.z - 2;
+    T* row = dst + ((int64_t)blockIdx.z * (n1 + 4) + blockIdx.y) * m0;
+    const bool row_in = (unsigned)i1 < (unsigned)n1 && (unsigned)i2 < (unsigned)n2;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < m0; p += gridDim.x * blockDim.x) {
+        const int i0 = p - 2;
+        row[p] = row_in && (unsigned)i0 < (unsigned)n0 ? src[i0 * s0 + i1 * s1 + i2 * s2] : T(0);
+    }
+}
+
+// Copy the volume into the caller's buffer with a zero border of two
+// texels per side (kk_fp_options.padded) and trace from its interior. The
+// paired loops need every offset from the interior, within
+// [-interior, total - interior), in 32 bits: larger volumes keep tracing
+// the volume itself.
+static int fp_pad_volume(FpArgs& L, const kk_volume* vol, const kk_fp_options* opts, cudaStream_t s,
+                         const char* who) {
+    int64_t n[3], st[3];
+    for (int k = 0; k < 3; ++k) {
+        n[L.rank[k]] = vol->shape[k];
+        st[L.rank[k]] = vol->stride[k];
+    }
+    const int64_t pst[3] = {1, n[0] + 4, (n[0] + 4) * (n[1] + 4)};
+    const int64_t total = pst[2] * (n[2] + 4);
+    if (opts->padded_elems < total)
+        return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: the padded copy needs %lld elements", who, (long long)total);
+    if (total >= ((int64_t)1 << 31) - 0x4B4000 - 2) return KK_OK;
+    const dim3 grid((unsigned)((n[0] + 4 + 255) / 256), (unsigned)(n[1] + 4), (unsigned)(n[2] + 4));
+    const int es = vol->dtype == KK_F32 ? 4 : 2;
+    if (es == 4)
+        fp_pad_kernel<float><<<grid, 256, 0, s>>>((const float*)vol->data, (float*)opts->padded, (int)n[0],
+                                                 (int)n[1], (int)n[2], st[0], st[1], st[2]);
+    else
+        fp_pad_kernel<unsigned short><<<grid, 256, 0, s>>>((const unsigned short*)vol->data,
+                                                           (unsigned short*)opts->padded, (int)n[0], (int)n[1],
+                                                           (int)n[2], st[0], st[1], st[2]);
+    const int64_t interior = 2 * (pst[0] + pst[1] + pst[2]);
+    L.vol = (const char*)opts->padded + interior * es;
+    for (int k = 0; k < 3; ++k) L.vs[k] = pst[L.rank[k]];
+    L.off32 = 1;
+    L.padded = 1;
+    return KK_OK;
 }
 
 static int fill_fp_args(FpArgs& L, const kk_volume* vol, const kk_projections* proj, const kk_fp_angle* angles,
@@ -1016,6 +1106,10 @@ extern "C" int kk_cone_fp_ex(const kk_volume* vol, const kk_projections* proj, c
         if ((vol->dtype == KK_F32) != (vtex->dtype == KK_F32))
             return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: texture and volume storage differ", who);
         L.vtex = vtex->tex;
+    }
+    if (opts->padded && tex8 && !(opts->flags & KK_FP_OPT_TILES)) {
+        rc = fp_pad_volume(L, vol, opts, (cudaStream_t)stream, who);
+        if (rc) return rc;
     }
     L.additive = opts->additive ? 1 : 0;
     if (opts->sums_elems < 0 || (opts->sums_elems > 0 && !opts->sums))

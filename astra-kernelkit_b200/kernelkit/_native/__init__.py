@@ -49,7 +49,8 @@ class kk_fp_options(ctypes.Structure):
                 ("additive", ctypes.c_int32), ("span", ctypes.c_int32),
                 ("flags", ctypes.c_int32), ("vtex", ctypes.c_void_p),
                 ("residual", ctypes.c_void_p), ("sums", ctypes.c_void_p),
-                ("sums_elems", ctypes.c_int64)]
+                ("sums_elems", ctypes.c_int64), ("padded", ctypes.c_void_p),
+                ("padded_elems", ctypes.c_int64)]
 
 
 #: kk_fp_options.flags: shared-memory tiles staged by the tensor-copy

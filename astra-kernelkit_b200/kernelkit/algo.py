@@ -379,8 +379,10 @@ class SIRT:
         self.R = R if not half else R.to(pdt)
         del R
         # make the forward projector's volume texture for the iterate's
-        # storage type now: it cannot be created during graph capture
+        # storage type now, and its padded volume copy: they cannot be
+        # created during graph capture
         self.fp._volume_texture(self.x, _native.volume_desc(self.x))
+        self.fp._padded(_native.volume_desc(self.x))
         self.y_tmp = t.empty_like(self.y)
         # the backprojection samples the residual through a layered
         # texture (the reference's filter), refilled every iteration

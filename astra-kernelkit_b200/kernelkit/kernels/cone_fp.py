@@ -130,6 +130,11 @@ class RayDrivenConeFP(BaseKernel):
     #: traced in chunks that fit it); 0 traces 16-bit projections in one
     #: launch
     sums_bytes = 1 << 30
+    #: texture-compatible weights: trace from a copy of the volume with two
+    #: zero texels around every axis, made at the start of every call
+    #: (same results; the CUDA-core rays of circular scans then sample the
+    #: slabs that cross the volume's boundary without per-texel tests)
+    padded_copy = True
 
     def __init__(self, pixels_per_block: tuple = None,
                  slices_per_block: int = None,
@@ -415,11 +420,31 @@ class RayDrivenConeFP(BaseKernel):
             self._sums_buf = buf
         return buf.data_ptr(), buf.numel()
 
-    def _options(self, lay, residual, additive, pdesc=None
+    def _padded(self, vdesc):
+        """(pointer, elements) of the zero-padded volume copy's buffer,
+        allocated once per projector, device, volume shape and type."""
+        if not self.padded_copy or self._interp != _native.KK_INTERP_TEX8:
+            return None, 0
+        t = _arrays.torch()
+        dt = {_native.KK_F32: t.float32, _native.KK_BF16: t.bfloat16,
+              _native.KK_F16: t.float16}[int(vdesc.dtype)]
+        n = int(np.prod([int(x) + 4 for x in vdesc.shape]))
+        buf = getattr(self, "_pad_buf", None)
+        dev = t.cuda.current_device()
+        if (buf is None or buf.numel() != n or buf.dtype != dt
+                or buf.device.index != dev):
+            self._pad_buf = None
+            buf = t.empty(n, dtype=dt, device="cuda")
+            self._pad_buf = buf
+        return buf.data_ptr(), buf.numel()
+
+    def _options(self, lay, residual, additive, pdesc=None, vdesc=None
                  ) -> "_native.kk_fp_options":
         o = _native.kk_fp_options()
         if pdesc is not None:
             o.sums, o.sums_elems = self._sums(pdesc)
+        if vdesc is not None:
+            o.padded, o.padded_elems = self._padded(vdesc)
         o.interp = self._interp if lay is None else _native.KK_INTERP_TEX8
         o.slab = self.slices_per_block
         o.additive = int(bool(additive))
@@ -433,7 +458,7 @@ class RayDrivenConeFP(BaseKernel):
         return o
 
     def _launch(self, vdesc, pdesc, osc, lay, residual, additive):
-        o = self._options(lay, residual, additive, pdesc)
+        o = self._options(lay, residual, additive, pdesc, vdesc)
         _native.check(_native.load().kk_cone_fp_ex(
             vdesc, pdesc, self._params_dev.data_ptr(), osc.ctypes.data, o,
             _native.current_stream()))

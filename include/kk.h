@@ -185,6 +185,20 @@ typedef struct {
                              pass through a 16-bit output unrounded.
                              Unused for float32 projections */
     int64_t sums_elems;   /* elements of sums */
+    void* padded;         /* NULL, or a device buffer of padded_elems
+                             elements of the volume's type, at least
+                             (n0 + 4)(n1 + 4)(n2 + 4) (no counterpart in the
+                             reference). With texture-compatible weights
+                             (and without KK_FP_OPT_TILES) the volume is
+                             copied into it at the start of the call with
+                             two zero texels before and after every axis,
+                             and the rays are traced from that copy: the
+                             CUDA-core rays of circular scans then sample
+                             slabs that cross the volume's boundary with
+                             the paired, test-free loads of the interior
+                             (the zeros are the border), not the per-ray
+                             checked loop. Same results bit for bit. */
+    int64_t padded_elems; /* elements of padded */
 } kk_fp_options;
 
 /* kk_fp_options.flags: rays traced on the CUDA cores sample shared-memory
