@@ -813,21 +813,26 @@ __global__ void __launch_bounds__(32 * FP_COLS, 4) cone_fp_batched_kernel(const 
 // ===========================================================================
 using namespace kk;
 
-// A projection with float32 output is traced in several launches of
-// FP_AUTO_SPAN slices of every ray's own slice axis (kk_fp_set_span sets
+// A projection with float32 output is traced in several launches of a
+// span of slices of every ray's own slice axis (kk_fp_set_span sets
 // another span, or one launch). Each launch then reads a band of the
 // volume across the rays' slice axes, whose slab per row tile stays in L2
 // (at 512^3 / 720 angles / 768^2: DRAM reads down, FP 183.0 -> 168.4 ms
 // with two launches; 64-slice spans lose to the per-launch ray set-up).
 // The running float32 sums are carried in the projections between
-// launches: same operations and rounding as one launch.
-constexpr int FP_AUTO_SPAN = 256;
+// launches: same operations and rounding as one launch. The automatic
+// span follows the longest axis, as measured with the padded-copy kernel:
+// one launch up to 256 slices (256^3 / 360 / 384^2: 9.7 ms, 10.4 ms with
+// 128 or 192), 192 up to 640 (512^3: 155.4 ms; 158.3 / 158.8 / 180.6 at
+// 128 / 256 / one launch), 128 beyond (1024^3 / 1440 / 1536^2: 2744 ms;
+// 2888 / 3059 / 3600 at 192 / 256 / one launch).
+static int fp_auto_span(int nmax) { return nmax <= 256 ? 256 : nmax <= 640 ? 192 : 128; }
 // span of the legacy entry points (kk_fp_set_span), per calling thread:
-// 0 = FP_AUTO_SPAN, < 0 = one launch, > 0 = slices
+// 0 = automatic (fp_auto_span), < 0 = one launch, > 0 = slices
 static thread_local int g_fp_span = 0;
 
 static int fp_span(int nmax, int slab, int setting) {
-    const int span = setting == 0 ? FP_AUTO_SPAN : setting;
+    const int span = setting == 0 ? fp_auto_span(nmax) : setting;
     if (span < 0 || span >= nmax) return 0;
     return (span + slab - 1) / slab * slab;
 }
@@ -968,17 +973,19 @@ static int launch_fp(const FpArgs& L, int vdt, int pdt, bool tex8, cudaStream_t 
 
 // The zero-padded copy: dst holds the volume with two zero texels before
 // and after every axis, in C order over the memory ranks (extents n[r] + 4,
-// rank 0 fastest); src has the volume's own strides (per rank). Block (x,
-// padded row along rank 1, padded plane along rank 2), threads along the
-// padded rank-0 row, so both sides stream.
+// rank 0 fastest); src has the volume's own strides (per rank). Block =
+// blockDim.y padded rows (rank 1) of one padded plane (rank 2, block y);
+// threads stride along the padded rank-0 row, so both sides stream.
 template <typename T>
 __global__ void fp_pad_kernel(const T* __restrict__ src, T* __restrict__ dst, int n0, int n1, int n2, int64_t s0,
                               int64_t s1, int64_t s2) {
-    const int m0 = n0 + 4;
-    const int i1 = (int)blockIdx.y - 2, i2 = (int)blockIdx.z - 2;
-    T* row = dst + ((int64_t)blockIdx.z * (n1 + 4) + blockIdx.y) * m0;
+    const int m0 = n0 + 4, m1 = n1 + 4;
+    const int r = blockIdx.x * blockDim.y + threadIdx.y;
+    if (r >= m1) return;
+    const int i1 = r - 2, i2 = (int)blockIdx.y - 2;
+    T* row = dst + ((int64_t)blockIdx.y * m1 + r) * m0;
     const bool row_in = (unsigned)i1 < (unsigned)n1 && (unsigned)i2 < (unsigned)n2;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < m0; p += gridDim.x * blockDim.x) {
+    for (int p = threadIdx.x; p < m0; p += blockDim.x) {
         const int i0 = p - 2;
         row[p] = row_in && (unsigned)i0 < (unsigned)n0 ? src[i0 * s0 + i1 * s1 + i2 * s2] : T(0);
     }
@@ -1001,13 +1008,13 @@ static int fp_pad_volume(FpArgs& L, const kk_volume* vol, const kk_fp_options* o
     if (opts->padded_elems < total)
         return kk_fail(KK_ERR_INVALID_ARGUMENT, "%s: the padded copy needs %lld elements", who, (long long)total);
     if (total >= ((int64_t)1 << 31) - 0x4B4000 - 2) return KK_OK;
-    const dim3 grid((unsigned)((n[0] + 4 + 255) / 256), (unsigned)(n[1] + 4), (unsigned)(n[2] + 4));
+    const dim3 block(128, 4), grid((unsigned)((n[1] + 4 + 3) / 4), (unsigned)(n[2] + 4));
     const int es = vol->dtype == KK_F32 ? 4 : 2;
     if (es == 4)
-        fp_pad_kernel<float><<<grid, 256, 0, s>>>((const float*)vol->data, (float*)opts->padded, (int)n[0],
-                                                 (int)n[1], (int)n[2], st[0], st[1], st[2]);
+        fp_pad_kernel<float><<<grid, block, 0, s>>>((const float*)vol->data, (float*)opts->padded, (int)n[0],
+                                                   (int)n[1], (int)n[2], st[0], st[1], st[2]);
     else
-        fp_pad_kernel<unsigned short><<<grid, 256, 0, s>>>((const unsigned short*)vol->data,
+        fp_pad_kernel<unsigned short><<<grid, block, 0, s>>>((const unsigned short*)vol->data,
                                                            (unsigned short*)opts->padded, (int)n[0], (int)n[1],
                                                            (int)n[2], st[0], st[1], st[2]);
     const int64_t interior = 2 * (pst[0] + pst[1] + pst[2]);

@@ -80,7 +80,8 @@ AXIS_GROUPS = (1, 2, 4, 8)
 #: fastest x middle volume axes swept together along the slowest)
 BP_TILES = ((8, 64), (4, 32), (8, 16), (2, 8))
 
-#: forward-projection slice spans tried (slices per launch; 0 = 256)
+#: forward-projection slice spans tried (slices per launch; 0 = the
+#: library's automatic span)
 FP_SPANS = (0, 96, 64)
 
 

@@ -542,9 +542,10 @@ _DEFAULT_SPAN = 0
 def set_slices_per_launch(slices: int = 0) -> None:
     """How many slices of every ray's own slice axis one forward-projection
     launch traces (float32 projections) for projectors that do not set
-    ``slices_per_launch`` themselves: 0 = the default (256), -1 = the
-    whole ray in one launch. Results are the same bit for bit; shorter
-    spans keep the volume band each launch reads in L2."""
+    ``slices_per_launch`` themselves: 0 = the library's automatic span
+    (one launch up to 256 slices, 192 slices up to 640, 128 beyond), -1 =
+    the whole ray in one launch. Results are the same bit for bit;
+    shorter spans keep the volume band each launch reads in L2."""
     global _DEFAULT_SPAN
     if int(slices) < -1:
         raise ValueError(f"slices must be >= -1, got {slices}")

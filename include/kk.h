@@ -157,8 +157,8 @@ KK_API int kk_cone_fp_layered(const kk_layered* vtex, const kk_volume* vol,
                               int32_t additive, void* stream);
 
 /* Options of kk_cone_fp_ex. A zero-initialised struct selects the
- * defaults: texture-compatible weights, 16-slice slabs, overwrite, 256-
- * slice spans, direct loads, no volume texture, no epilogue. */
+ * defaults: texture-compatible weights, 16-slice slabs, overwrite,
+ * automatic slice spans, direct loads, no volume texture, no epilogue. */
 typedef struct {
     int32_t interp;     /* kk_interp */
     int32_t slab;       /* slices per coordinate restart; <= 0 selects 16 */
@@ -170,8 +170,10 @@ typedef struct {
                            to the slab; the running float32 sums are carried
                            in the projections, so the result is bit for bit
                            that of one launch) and each launch reads a band
-                           of the volume that stays in L2. 0: 256 slices,
-                           -1: one launch */
+                           of the volume that stays in L2. 0: by the
+                           longest axis (one launch up to 256 slices, 192-
+                           slice spans up to 640, 128 beyond), -1: one
+                           launch */
     int32_t flags;      /* KK_FP_OPT_* bits */
     const kk_layered* vtex;          /* NULL, or a layered copy of the
                                         volume as for kk_cone_fp_layered */
@@ -223,7 +225,7 @@ KK_API int kk_cone_fp_ex(const kk_volume* vol, const kk_projections* proj,
 
 /* Launch split of kk_cone_fp, kk_cone_fp_residual and kk_cone_fp_layered,
  * as kk_fp_options.span, for the calling thread (each thread starts with
- * 0 = 256 slices; -1 selects one launch). */
+ * 0 = automatic, as kk_fp_options.span; -1 selects one launch). */
 KK_API int kk_fp_set_span(int32_t slices);
 
 /* Number of kernel launches kk_cone_fp* makes for a volume whose longest
@@ -345,7 +347,7 @@ typedef struct {
     kk_fp_residual residual;    /* y and weight NULL: plain projection */
     int32_t additive;
     int32_t span;               /* slices per launch, as kk_fp_options.span
-                                   (0: 256, -1: one launch) */
+                                   (0: automatic, -1: one launch) */
 } kk_fp_problem;
 
 /* kk_cone_fp / kk_cone_fp_layered / kk_cone_fp_residual for n problems

@@ -88,17 +88,19 @@ def test_interpolation_mode_checked():
 
 def test_fp_launch_split_is_host_logic():
     """kk_fp_launches / kk_fp_set_span (no GPU needed): float32 projections
-    of volumes longer than 256 slices are traced in 256-slice launches by
-    default; 16-bit projections in one launch, unless a float32
-    running-sum buffer carries the sums (then per chunk of angles)."""
+    are traced in one launch up to 256 slices, in 192-slice launches up to
+    640 and in 128-slice launches beyond by default; 16-bit projections in
+    one launch, unless a float32 running-sum buffer carries the sums (then
+    per chunk of angles)."""
     from kernelkit.kernels.cone_fp import (launches_per_projection,
                                            set_slices_per_launch)
 
     assert launches_per_projection(256) == 1
-    assert launches_per_projection(512) == 2
-    assert launches_per_projection(1024) == 4
+    assert launches_per_projection(384) == 2
+    assert launches_per_projection(512) == 3
+    assert launches_per_projection(1024) == 8
     assert launches_per_projection(1024, float32=False) == 1
-    assert launches_per_projection(1024, float32=False, sums=True) == 4
+    assert launches_per_projection(1024, float32=False, sums=True) == 8
     L = _native.load()
     assert L.kk_fp_launches(1024, 16, _native.KK_F16) == 1
     try:
