@@ -104,6 +104,7 @@ BP_ANGLE_DTYPE = np.dtype([("num_u", "<f4", 4), ("num_v", "<f4", 4),
 
 #: every symbol include/kk.h declares
 EXPORTS = ("kk_cone_fp_ex", "kk_fp_launches_ex", "kk_wait_timeouts",
+           "kk_bp_launches",
            "kk_fdk_filter", "kk_fdk_plan", "kk_fdk_plan_size",
            "kk_cone_bp_layered_batched_ex", "kk_bp_batch_sync_elems",
            "kk_cone_fp", "kk_cone_fp_residual", "kk_cone_fp_layered",
@@ -140,6 +141,8 @@ def load():
     L.kk_cone_fp_ex.argtypes = [P(kk_volume), P(kk_projections), vp, vp,
                                 P(kk_fp_options), vp]
     L.kk_fp_launches_ex.argtypes = [i32, i32, i32, i32]
+    L.kk_bp_launches.argtypes = [i64]
+    L.kk_bp_launches.restype = i32
     L.kk_wait_timeouts.argtypes = [P(i32)]
     L.kk_cone_fp.argtypes = [P(kk_volume), P(kk_projections), vp, vp, i32,
                              i32, i32, vp]

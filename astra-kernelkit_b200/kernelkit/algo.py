@@ -139,8 +139,9 @@ def _streamed_bp(projections: np.ndarray, projection_geometry,
                  volume_geometry: VolumeGeometry, filter: Any,
                  kernel: VoxelDrivenConeBP = None):
     """Backprojection (with FDK pre-weighting and filtering when ``filter``
-    is given) in 32-angle chunks through a two-slot ring of 32-layer
-    textures, so no whole-scan texture is allocated. Host projections are
+    is given) in stages of 32 angles (host input) or 128 angles (device
+    input) through a two-slot ring of textures, so no whole-scan texture
+    is allocated. Host projections are
     streamed: while the host stages chunk c+1 into pinned memory and a
     copy stream uploads it, the GPU pre-weights and filters chunk c,
     copies it into a texture and backprojects it onto the volume; the
@@ -201,8 +202,12 @@ def _streamed_bp(projections: np.ndarray, projection_geometry,
             d, pw.data_ptr() + a * 13 * 8, plan.data_ptr(), P,
             d if in_place else None, tex.handle, 0, stream))
     staged, used = [None, None], [None, None]
-    for c, a in enumerate(range(0, n, _CHUNK)):
-        m, b = min(_CHUNK, n - a), c & 1
+    # device input: four chunks per stage, so that each BP launch covers
+    # four 32-angle chunks (added one by one, as in the whole-scan path);
+    # host input: one chunk per stage, for a finer overlap with the copies
+    step = _CHUNK if on_host else 4 * _CHUNK
+    for c, a in enumerate(range(0, n, step)):
+        m, b = min(step, n - a), c & 1
         texs = st["tex"].get(m)
         if texs is None:
             texs = [_native.Layered(m, rows, cols, _native.KK_F32)

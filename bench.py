@@ -894,6 +894,8 @@ def run_ours(args):
     # cone_fp_pad_kernel, or the volume itself with cone_fp_kernel
     fp_name = "cone_fp_pad_kernel" if fp.padded_copy else "cone_fp_kernel"
     pad_launches = 1 if fp.padded_copy else 0
+    # one BP launch per four 32-angle chunks
+    bp_launches = int(_native.load().kk_bp_launches(len(pgs)))
     fp_bytes = 4.0 * nupd  # algorithmic: one float32 voxel operand / update
     roofline = {"kernel": fp_name, "bound": "hbm",
                 "achieved": fp_bytes / (t_fp * 1e-3) / 1e9, "peak": peak,
@@ -929,7 +931,7 @@ def run_ours(args):
                   "gups": nupd / (t_fp * 1e-3) / 1e9,
                   "achieved_gbs": fp_bytes / (t_fp * 1e-3) / 1e9,
                   "traffic": load_traffic(args.workload, fp_name)},
-        "cone_bp_kernel": {"ms": t_bp, "launches": (len(pgs) + 31) // 32,
+        "cone_bp_kernel": {"ms": t_bp, "launches": bp_launches,
                            "gups": nupd / (t_bp * 1e-3) / 1e9,
                            "achieved_gbs": fp_bytes / (t_bp * 1e-3) / 1e9,
                            "traffic": load_traffic(args.workload,
@@ -992,10 +994,10 @@ def run_ours(args):
             "e2e": e2e, "roofline": roofline,
             "texture_roofline": texture_roofline, "cpu_baseline": cpu,
             "kernels": kernels, "reference_kernels": refk,
-            # per step: the FP's padded copy and slice-span launches, one
-            # BP launch per 32-angle chunk
+            # per step: the FP's padded copy and slice-span launches, the
+            # BP's launches (four 32-angle chunks each)
             "gpu_launches": args.steps * (pad_launches + fp_launches
-                                          + (len(pgs) + 31) // 32),
+                                          + bp_launches),
             "clocks": clocks, "fdk": fdk, "sirt": sirt, "batched": batched,
         }
         print(json.dumps(line), flush=True)

@@ -294,9 +294,16 @@ KK_API int kk_cone_bp_static(const kk_projections* proj, const kk_volume* vol,
                              const kk_bp_angle* angles, float out_scale,
                              int32_t interp, int32_t additive, void* stream);
 
+/* Kernel launches of kk_cone_bp / kk_cone_bp_layered / kk_cone_bp_update
+ * for n_angles angles when the running sum has a home (a float32 volume
+ * or a work buffer): one per four 32-angle chunks, each chunk still added
+ * to the running sum on its own (no counterpart in the reference, which
+ * launches once per chunk). */
+KK_API int32_t kk_bp_launches(int64_t n_angles);
+
 /* Backprojection fused with the SIRT update epilogue (kk_bp_update); work
  * as for kk_cone_bp (the update needs it whenever there are more than 32
- * angles, to keep one launch per chunk). */
+ * angles, to keep one launch per chunk group). */
 KK_API int kk_cone_bp_update(const kk_projections* proj, const kk_volume* vol,
                              const kk_bp_angle* angles, float out_scale,
                              const kk_bp_update* update, int32_t interp,

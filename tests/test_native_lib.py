@@ -86,6 +86,14 @@ def test_interpolation_mode_checked():
     assert b"interpolation" in L.kk_last_error()
 
 
+def test_bp_launch_count_is_host_logic():
+    """kk_bp_launches (no GPU needed): one launch per four 32-angle
+    chunks."""
+    L = _native.load()
+    assert [L.kk_bp_launches(n) for n in (0, 1, 32, 128, 129, 720, 1440)] \
+        == [0, 1, 1, 1, 2, 6, 12]
+
+
 def test_fp_launch_split_is_host_logic():
     """kk_fp_launches / kk_fp_set_span (no GPU needed): float32 projections
     are traced in one launch up to 256 slices, in 192-slice launches up to
