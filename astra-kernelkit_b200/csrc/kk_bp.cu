@@ -199,8 +199,8 @@ __global__ void __launch_bounds__(BP_TILE_2* BP_TILE_1) cone_bp_batched_kernel(c
     const int tx = B.tiles[i][0], ty = B.tiles[i][1];
     const int tz = (B.block_start[i + 1] - B.block_start[i]) / (tx * ty);
     int bx, by, bz;
-    bp_tile_order(t, tx, ty, tz, bx, by, bz, Ls.tile_z > 0 ? Ls.tile_z : KK_BP_TILE_Z,
-                  Ls.tile_y > 0 ? Ls.tile_y : KK_BP_TILE_Y);
+    // one chunk per launch here: the one-chunk super-column default
+    bp_tile_order(t, tx, ty, tz, bx, by, bz, Ls.tile_z > 0 ? Ls.tile_z : 8, Ls.tile_y > 0 ? Ls.tile_y : 64);
     bp_block<float, float, true, EPI, FETCH_TEX>(Ls, bx, by, bz);
 }
 
