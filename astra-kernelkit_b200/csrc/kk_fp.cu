@@ -25,14 +25,20 @@ namespace kk {
 // column sees the same D1 coordinate sequence, bit for bit, and the D1
 // split is done once per slice for the thread's rows. Otherwise a generic
 // per-ray path with arbitrary strides is used.
+#ifndef KK_FP_COLS
+// 4 columns (128-thread blocks, twice the blocks per SM at the same
+// registers): 155.5 -> 152.9 ms at the 512^3 x 720 x 768^2 scan, whose
+// SMs then mix texture and CUDA-core blocks more finely; 16: 181 ms
+#define KK_FP_COLS 4
+#endif
 #ifndef KK_FP_RPT
 #define KK_FP_RPT 2
 #endif
 #ifndef KK_FP_MINBLOCKS
-#define KK_FP_MINBLOCKS 6
+#define KK_FP_MINBLOCKS (48 / KK_FP_COLS)  // 40 registers
 #endif
 #ifndef KK_FP_PAD_MINBLOCKS
-#define KK_FP_PAD_MINBLOCKS 5  // the padded-copy kernel: 48 registers, no spills
+#define KK_FP_PAD_MINBLOCKS (40 / KK_FP_COLS)  // the padded-copy kernel: 48 registers, no spills
 #endif
 #ifndef KK_FP_PAD_TEX_UNROLL
 #define KK_FP_PAD_TEX_UNROLL 8  // its texture loop (4 in the 40-register kernel)
@@ -47,7 +53,7 @@ constexpr int FP_RPT = KK_FP_RPT;       // rays per thread
 constexpr int FP_UNROLL = KK_FP_UNROLL;
 constexpr int FP_TEX_UNROLL = KK_FP_TEX_UNROLL;
 constexpr int FP_PAD_TEX_UNROLL = KK_FP_PAD_TEX_UNROLL;
-constexpr int FP_COLS = 8;              // columns per block (one per warp)
+constexpr int FP_COLS = KK_FP_COLS;     // columns per block (one per warp)
 constexpr int FP_ROWS_T = 32 * FP_RPT;  // rows per block
 
 // Bilinear sample times weight_unit() on a plane whose D2 axis has unit
@@ -793,7 +799,7 @@ struct FpBatch {
 };
 
 template <bool TEX8, int EPI>
-__global__ void __launch_bounds__(32 * FP_COLS, 4) cone_fp_batched_kernel(const __grid_constant__ FpBatch B) {
+__global__ void __launch_bounds__(32 * FP_COLS, 32 / FP_COLS) cone_fp_batched_kernel(const __grid_constant__ FpBatch B) {
     __shared__ FpArgs Ls;
     const int b = blockIdx.x;
     int i = 0;
