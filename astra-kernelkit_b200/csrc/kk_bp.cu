@@ -207,27 +207,31 @@ __global__ void __launch_bounds__(BP_TILE_2* BP_TILE_1) cone_bp_batched_kernel(c
 // ---------------------------------------------------------------------------
 // persistent batched backprojection
 // ---------------------------------------------------------------------------
-// One grid of resident blocks works through every (chunk, problem, tile)
-// item of a batch: a block claims the next item from a counter in global
-// memory, items ordered by chunk index first, so every chunk of a tile is
-// claimed after the tile's previous chunk. An item of chunk c > 0 starts
-// from the running sums its tile's chunk c - 1 left behind: it waits until
-// the tile's counter says c chunks are done (spinning with a clock64()
+// One grid of resident blocks works through every (chunk group, problem,
+// tile) item of a batch, a group being BP_PERSIST_GROUP consecutive
+// 32-angle chunks that one item backprojects with its running sum in
+// registers (each chunk still added on its own, as in the other paths): a
+// block claims the next item from a counter in global memory, items
+// ordered by group index first, so every group of a tile is claimed after
+// the tile's previous group. An item of group c > 0 starts from the
+// running sums its tile's group c - 1 left behind: it waits until the
+// tile's counter says c groups are done (spinning with a clock64()
 // budget; a wait that runs out records a timeout, raises the abort flag
 // and skips the item, and every block stops claiming), runs the same
 // block code as the one-launch-per-chunk path, then publishes c + 1. The
 // item that is waited on was claimed earlier by a running block, which
 // itself only waits on still earlier items, so the waits always end.
 constexpr int BP_MAX_CHUNKS = 64;  // 2048 angles, the layered-texture limit
+constexpr int BP_PERSIST_GROUP = 4;  // 32-angle chunks per item
 
 struct BpSched {
     int n;       // problems
-    int chunks;  // largest chunk count
+    int chunks;  // largest chunk-group count
     int items;
     int skip_item;  // tests of the bounded wait: this item is never run
     long long budget;
-    int cstart[BP_MAX_CHUNKS + 1];  // first item of each chunk index
-    int nchunks[KK_MAX_BATCH];
+    int cstart[BP_MAX_CHUNKS + 1];  // first item of each group index
+    int nchunks[KK_MAX_BATCH];      // chunk groups per problem
     int tiles[KK_MAX_BATCH];
     int grid[KK_MAX_BATCH][3];
     int tile_base[KK_MAX_BATCH];  // first counter of each problem
@@ -275,8 +279,8 @@ __global__ void __launch_bounds__(BP_TILE_2* BP_TILE_1) cone_bp_persistent_kerne
                 }
             }
             __threadfence();  // the previous chunk's sums before ours
-            Ls.j_begin = c * BP_CHUNK;
-            Ls.j_end = min(Ls.n_angles, Ls.j_begin + BP_CHUNK);
+            Ls.j_begin = c * BP_CHUNK * BP_PERSIST_GROUP;
+            Ls.j_end = min(Ls.n_angles, Ls.j_begin + BP_CHUNK * BP_PERSIST_GROUP);
             const bool update = Ls.upd_scale != nullptr;
             const bool need_work = S.nchunks[p] > 1 && update;  // float32 volumes
             const int first_load = (Ls.additive && !update) ? LOAD_VOL : LOAD_ZERO;
@@ -288,8 +292,8 @@ __global__ void __launch_bounds__(BP_TILE_2* BP_TILE_1) cone_bp_persistent_kerne
         __syncthreads();
         if (s_go) {
             int bx, by, bz;
-            bp_tile_order(t, S.grid[p][0], S.grid[p][1], S.grid[p][2], bx, by, bz, Ls.tile_z > 0 ? Ls.tile_z : 8,
-                          Ls.tile_y > 0 ? Ls.tile_y : 64);
+            bp_tile_order(t, S.grid[p][0], S.grid[p][1], S.grid[p][2], bx, by, bz,
+                          Ls.tile_z > 0 ? Ls.tile_z : KK_BP_TILE_Z, Ls.tile_y > 0 ? Ls.tile_y : KK_BP_TILE_Y);
             if (Ls.upd_scale)
                 bp_block<float, float, true, BP_UPDATE, FETCH_TEX>(Ls, bx, by, bz);
             else
@@ -726,6 +730,9 @@ extern "C" int kk_cone_bp_layered_batched_ex(const kk_bp_problem* pr, int32_t n,
     static BpSched S;  // host staging, copied into the launch parameters
     static std::mutex S_mutex;
     std::lock_guard<std::mutex> lock(S_mutex);
+    // items of BP_PERSIST_GROUP chunks
+    for (int i = 0; i < n; ++i) chunks[i] = (chunks[i] + BP_PERSIST_GROUP - 1) / BP_PERSIST_GROUP;
+    max_chunks = (max_chunks + BP_PERSIST_GROUP - 1) / BP_PERSIST_GROUP;
     S.n = n;
     S.chunks = max_chunks;
     S.skip_item = opts->test_skip_item;

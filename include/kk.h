@@ -405,11 +405,13 @@ typedef struct {
 } kk_bp_batch_options;
 
 /* The batched backprojection as ONE persistent launch (no counterpart in
- * the reference): resident thread blocks claim (chunk, problem, tile)
- * items, chunk index first, from a counter; an item of chunk c of a tile
- * waits (bounded) for the tile's chunk c - 1, then adds its 32 angles to
- * the running sums with the same block code, so results equal
- * kk_cone_bp_layered_batched bit for bit. Float32 volumes. */
+ * the reference): resident thread blocks claim (chunk group, problem,
+ * tile) items, group index first, from a counter, a group being four
+ * consecutive 32-angle chunks; an item of group c of a tile waits
+ * (bounded) for the tile's group c - 1, then adds its chunks' angles to
+ * the running sums one chunk at a time with the same block code, so
+ * results equal kk_cone_bp_layered_batched bit for bit. Float32
+ * volumes. */
 KK_API int kk_cone_bp_layered_batched_ex(const kk_bp_problem* problems,
                                          int32_t n,
                                          const kk_bp_batch_options* opts,

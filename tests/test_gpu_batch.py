@@ -187,10 +187,11 @@ def _bp_batch(cases, update=False):
 
 @pytest.mark.parametrize("update", [False, True])
 def test_persistent_backprojection_equals_per_chunk_launches(update):
-    """One persistent launch walking (chunk, problem, tile) items gives the
-    per-chunk-index launches' volumes bit for bit (96-, 24-, 18- and
-    12-angle scans: 3, 1, 1 and 1 chunks)."""
-    cases = ("config1", "small", "alldirs", "volrot")
+    """One persistent launch walking (chunk group, problem, tile) items
+    gives the per-chunk-index launches' volumes bit for bit (360-, 96-,
+    24-, 18- and 12-angle scans: 12, 3, 1, 1 and 1 chunks, i.e. 3, 1, 1, 1
+    and 1 groups of four, so items of later groups wait on earlier ones)."""
+    cases = ("config2", "config1", "small", "alldirs", "volrot")
     arr, ref, keep = _bp_batch(cases, update)
     start = [o.clone() for o in ref]
     _native.check(_native.load().kk_cone_bp_layered_batched(
@@ -215,9 +216,11 @@ def test_persistent_backprojection_equals_per_chunk_launches(update):
 
 def test_persistent_backprojection_wait_runs_out():
     """An item that never completes (a flag nothing sets): the item of the
-    tile's next chunk waits out a short budget, the launch aborts instead
-    of hanging and the host reads the timeout; the library keeps working."""
-    cases = ("config1", "small")
+    tile's next chunk group waits out a short budget, the launch aborts
+    instead of hanging and the host reads the timeout; the library keeps
+    working. The first problem has more than one group of four 32-angle
+    chunks (config 2: 360 angles), so a later item waits on item 0."""
+    cases = ("config2", "small")
     arr, outs, keep = _bp_batch(cases)
     L = _native.load()
     elems = int(L.kk_bp_batch_sync_elems(arr, len(cases)))
