@@ -5,9 +5,10 @@ solved together: every SIRT iteration of every problem is one batched
 forward-projection launch (``kk_cone_fp_batched``: up to 64 problems per
 launch, each thread block picking its own problem), the texture refills,
 and one persistent backprojection launch (``kk_cone_bp_layered_batched_ex``:
-resident thread blocks claim (chunk, problem, tile) items in chunk order,
-each waiting with a bounded spin for its tile's previous chunk) or, with
-``persistent=False``, one launch per 32-angle chunk index. The whole
+resident thread blocks claim (chunk group, problem, tile) items in group
+order, a group being four 32-angle chunks, each waiting with a bounded
+spin for its tile's previous group) or, with ``persistent=False``, one
+launch per 32-angle chunk index. The whole
 iteration sequence can be captured in one CUDA graph. Launch-shape
 choices (the forward projector's record grouping, the backprojection's
 super-column shape, the slice span per launch) are made per problem
